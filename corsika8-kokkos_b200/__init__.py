@@ -1,0 +1,340 @@
+"""B200 radio projection (CoREAS endpoint field + ZHS vector potential).
+
+Python view of libc8radio.so, the sm_100a drop-in for the CORSIKA8-kokkos
+radio accumulator (corsika/kokkos/radio/RadioAccumulator.hpp).  Names and
+argument meaning follow the reference: a RadioConfig with CoREAS and ZHS
+observer snapshots and a flat-atmosphere refractivity table, a
+RadioAccumulator fed LeptonTransportRecord batches from host or device
+memory, and download()/download_fixed() returning the traces.  Failures raise
+the Python counterparts of the reference's exception classes.
+
+There is no CPU fallback: every call runs the CUDA library, and loading the
+package without the built library raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from pathlib import Path
+from typing import Optional
+
+import numpy as np
+
+from . import abi
+from .abi import LEPTON_RECORD, OBSERVER, PARTICLE_STATE  # noqa: F401
+
+HERE = Path(__file__).resolve().parent
+LIBRARY_PATH = HERE / "libc8radio.so"
+
+# ------------------------------------------------------------------ errors
+class RadioError(RuntimeError):
+    """Base class of radio failures reported by the C boundary."""
+
+
+class InvalidArgument(RadioError, ValueError):
+    """std::invalid_argument"""
+
+
+class LogicError(RadioError):
+    """std::logic_error"""
+
+
+class OutOfRange(RadioError, IndexError):
+    """std::out_of_range"""
+
+
+class FixedPointOverflow(RadioError):
+    """std::runtime_error raised at download when the fixed-point traces overflowed"""
+
+
+class LengthError(RadioError):
+    """std::length_error"""
+
+
+class OverflowErrorRadio(RadioError, OverflowError):
+    """std::overflow_error"""
+
+
+class CudaError(RadioError):
+    """CUDA runtime failure"""
+
+
+class AllocationError(RadioError, MemoryError):
+    """device or pinned allocation failure"""
+
+
+_STATUS = {
+    abi.C8R_INVALID_ARGUMENT: InvalidArgument,
+    abi.C8R_LOGIC_ERROR: LogicError,
+    abi.C8R_OUT_OF_RANGE: OutOfRange,
+    abi.C8R_RUNTIME_ERROR: FixedPointOverflow,
+    abi.C8R_LENGTH_ERROR: LengthError,
+    abi.C8R_OVERFLOW_ERROR: OverflowErrorRadio,
+    abi.C8R_CUDA_ERROR: CudaError,
+    abi.C8R_BAD_ALLOC: AllocationError,
+}
+
+_lib: Optional[C.CDLL] = None
+
+
+def library() -> C.CDLL:
+    """Loads libc8radio.so (building it first if sources are newer)."""
+    global _lib
+    if _lib is None:
+        if not LIBRARY_PATH.exists():
+            from . import build as _build
+
+            _build.build()
+        if not LIBRARY_PATH.exists():
+            raise ImportError(f"libc8radio.so is missing at {LIBRARY_PATH}; run build.py")
+        _lib = abi.bind(C.CDLL(str(LIBRARY_PATH)))
+    return _lib
+
+
+def _raise(status: int, message: bytes | None) -> None:
+    if status == abi.C8R_OK:
+        return
+    text = (message or b"").decode(errors="replace")
+    raise _STATUS.get(status, RadioError)(text or f"radio status {status}")
+
+
+# ------------------------------------------------------------------ config
+@dataclass
+class FlatAtmosphereSnapshot:
+    """corsika/kokkos/radio/FlatAtmosphereRadioSnapshot.hpp:20-36"""
+
+    homogeneous_refractive_index: float = 0.0
+    minimum_height_m: float = 0.0
+    maximum_height_m: float = 0.0
+    step_m: float = 0.0
+    inverse_step_per_m: float = 0.0
+    slope_refractivity_lower: float = 0.0
+    slope_integrated_refractivity_lower: float = 0.0
+    slope_refractivity_upper: float = 0.0
+    slope_integrated_refractivity_upper: float = 0.0
+    refractivity: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    integrated_refractivity: np.ndarray = field(default_factory=lambda: np.zeros(0))
+
+
+@dataclass
+class RadioConfig:
+    """corsika/kokkos/radio/RadioConfig.hpp:21-53 plus the B200 precision/kernel choice."""
+
+    enabled: bool = False
+    coreas_enabled: bool = True
+    zhs_enabled: bool = True
+    deterministic: bool = True
+    fixed_point_field_limit_v_per_m: float = 1.0
+    track_diagnostics: bool = False
+    zhs_subtrack_refinement: int = 1
+    propagation: FlatAtmosphereSnapshot = field(default_factory=FlatAtmosphereSnapshot)
+    coreas_observers: np.ndarray = field(default_factory=lambda: np.zeros(0, OBSERVER))
+    zhs_observers: np.ndarray = field(default_factory=lambda: np.zeros(0, OBSERVER))
+    precision: int = abi.PRECISION_FP64
+    kernel: int = abi.KERNEL_AUTO
+
+    def to_c(self):
+        """Returns (abi.Config, keepalive) with pointers into contiguous copies."""
+        keep = []
+        p = self.propagation
+        n = np.ascontiguousarray(p.refractivity, dtype=np.float64)
+        i = np.ascontiguousarray(p.integrated_refractivity, dtype=np.float64)
+        co = np.ascontiguousarray(self.coreas_observers, dtype=OBSERVER)
+        zo = np.ascontiguousarray(self.zhs_observers, dtype=OBSERVER)
+        keep += [n, i, co, zo]
+        dptr = C.POINTER(C.c_double)
+        prop = abi.PropagationSnapshot(
+            p.homogeneous_refractive_index, p.minimum_height_m, p.maximum_height_m, p.step_m,
+            p.inverse_step_per_m, p.slope_refractivity_lower,
+            p.slope_integrated_refractivity_lower, p.slope_refractivity_upper,
+            p.slope_integrated_refractivity_upper,
+            n.ctypes.data_as(dptr) if n.size else dptr(),
+            i.ctypes.data_as(dptr) if i.size else dptr(),
+            int(n.size),
+        )
+        cfg = abi.Config(
+            int(self.enabled), int(self.coreas_enabled), int(self.zhs_enabled),
+            int(self.deterministic), float(self.fixed_point_field_limit_v_per_m),
+            int(self.track_diagnostics), int(self.zhs_subtrack_refinement), prop,
+            co.ctypes.data if co.size else None, int(co.size),
+            zo.ctypes.data if zo.size else None, int(zo.size),
+            int(self.precision), int(self.kernel),
+        )
+        return cfg, keep
+
+
+@dataclass
+class TuningParameters:
+    """corsika/kokkos/runtime/TuningParameters.hpp:14-21 (zero keeps defaults).
+
+    batch_size: host staging batch (records); team_size: threads per windowed
+    CTA; track_tile_size: tracks per windowed work item; observer_tile_size:
+    shared-memory window (bins)."""
+
+    batch_size: int = 0
+    chunk_size: int = 0
+    team_size: int = 0
+    track_tile_size: int = 0
+    observer_tile_size: int = 0
+    device_queues: int = 1
+
+    def to_c(self) -> abi.Tuning:
+        return abi.Tuning(self.batch_size, self.chunk_size, self.team_size,
+                          self.track_tile_size, self.observer_tile_size, self.device_queues)
+
+
+def validate(config: RadioConfig) -> None:
+    lib = library()
+    cfg, keep = config.to_c()
+    _raise(lib.c8r_config_validate(C.byref(cfg)), lib.c8r_last_global_error())
+
+
+def projected_device_bytes(config: RadioConfig) -> int:
+    lib = library()
+    cfg, keep = config.to_c()
+    out = C.c_size_t()
+    _raise(lib.c8r_projected_device_bytes(C.byref(cfg), C.byref(out)), lib.c8r_last_global_error())
+    return out.value
+
+
+@dataclass
+class RadioWaveforms:
+    """corsika/kokkos/radio/RadioWaveforms.hpp:19-22: CoREAS E (V/m) and ZHS A (V s/m),
+    each a (3, total_bins) array in the accumulator's SoA order; split per
+    observer with `observer_traces`."""
+
+    coreas: np.ndarray
+    zhs: np.ndarray
+    counters: dict
+
+
+def observer_traces(traces: np.ndarray, observers: np.ndarray) -> list:
+    out, offset = [], 0
+    for n in observers["number_of_bins"]:
+        out.append(traces[:, offset:offset + int(n)])
+        offset += int(n)
+    return out
+
+
+class RadioAccumulator:
+    """corsika::kokkos::radio::RadioAccumulator over libc8radio.so.
+
+    stream: an integer cudaStream_t handle (e.g. torch.cuda.Stream().cuda_stream)
+    or None for the legacy default stream."""
+
+    def __init__(self, config: RadioConfig, tuning: Optional[TuningParameters] = None,
+                 stream: Optional[int] = None):
+        self._lib = library()
+        self.config = config
+        cfg, self._keep = config.to_c()
+        t = (tuning or TuningParameters()).to_c()
+        handle = C.c_void_p()
+        status = self._lib.c8r_create(C.byref(cfg), C.byref(t), C.c_void_p(stream or 0),
+                                      C.byref(handle))
+        _raise(status, self._lib.c8r_last_global_error())
+        self._h = handle
+        cb, zb = C.c_size_t(), C.c_size_t()
+        self._check(self._lib.c8r_total_bins(self._h, C.byref(cb), C.byref(zb)))
+        self.coreas_bins, self.zhs_bins = cb.value, zb.value
+
+    def _check(self, status: int) -> None:
+        if status != abi.C8R_OK:
+            _raise(status, self._lib.c8r_last_error(self._h))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.c8r_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # reference method set -------------------------------------------------
+    def enabled(self) -> bool:
+        out = C.c_int()
+        self._check(self._lib.c8r_enabled(self._h, C.byref(out)))
+        return bool(out.value)
+
+    def reset(self) -> None:
+        self._check(self._lib.c8r_reset(self._h))
+
+    def enqueue_host_lepton_tracks(self, records: Optional[np.ndarray]) -> None:
+        if records is None:
+            self._check(self._lib.c8r_enqueue_host(self._h, None, 0))
+            return
+        records = np.ascontiguousarray(records, dtype=LEPTON_RECORD)
+        self._check(self._lib.c8r_enqueue_host(self._h, records.ctypes.data, records.size))
+
+    def enqueue_host_pointer(self, pointer: Optional[int], count: int) -> None:
+        """Raw form of enqueueHostLeptonTracks (a NULL pointer with count > 0 is rejected)."""
+        self._check(self._lib.c8r_enqueue_host(self._h, pointer, count))
+
+    def flush_host_lepton_tracks(self) -> None:
+        self._check(self._lib.c8r_flush(self._h))
+
+    def accumulate_lepton_tracks(self, device_pointer: int, count: int,
+                                 extent: Optional[int] = None) -> None:
+        """accumulateLeptonTracks on records in device memory (stream ordered)."""
+        self._check(self._lib.c8r_accumulate_device(
+            self._h, C.c_void_p(device_pointer), count, count if extent is None else extent))
+
+    def download(self) -> RadioWaveforms:
+        coreas = np.zeros((3, self.coreas_bins), np.float64)
+        zhs = np.zeros((3, self.zhs_bins), np.float64)
+        counters = abi.Counters()
+        self._check(self._lib.c8r_download(
+            self._h, coreas.ctypes.data if coreas.size else None,
+            zhs.ctypes.data if zhs.size else None, C.byref(counters)))
+        return RadioWaveforms(coreas, zhs, counters.as_dict())
+
+    def download_into(self, coreas: Optional[np.ndarray], zhs: Optional[np.ndarray]) -> dict:
+        """download() into caller-owned (e.g. pinned) float64 buffers of 3*bins."""
+        counters = abi.Counters()
+        self._check(self._lib.c8r_download(
+            self._h, None if coreas is None else coreas.ctypes.data,
+            None if zhs is None else zhs.ctypes.data, C.byref(counters)))
+        return counters.as_dict()
+
+    def download_fixed(self):
+        coreas = np.zeros((3, self.coreas_bins), np.int64)
+        zhs = np.zeros((3, self.zhs_bins), np.int64)
+        counters = abi.Counters()
+        self._check(self._lib.c8r_download_fixed(
+            self._h, coreas.ctypes.data if coreas.size else None,
+            zhs.ctypes.data if zhs.size else None, C.byref(counters)))
+        return coreas, zhs, counters.as_dict()
+
+    def statistics(self) -> abi.Statistics:
+        s = abi.Statistics()
+        self._check(self._lib.c8r_get_statistics(self._h, C.byref(s)))
+        return s
+
+    def device_bytes(self) -> int:
+        out = C.c_size_t()
+        self._check(self._lib.c8r_device_bytes(self._h, C.byref(out)))
+        return out.value
+
+    def static_host_to_device_bytes(self) -> int:
+        out = C.c_size_t()
+        self._check(self._lib.c8r_static_host_to_device_bytes(self._h, C.byref(out)))
+        return out.value
+
+    def reserve_track_capacity(self, count: int) -> None:
+        self._check(self._lib.c8r_reserve(self._h, count))
+
+    def projected_track_capacity(self, count: int):
+        r, p = C.c_size_t(), C.c_size_t()
+        self._check(self._lib.c8r_projected_track_capacity(self._h, count, C.byref(r), C.byref(p)))
+        return r.value, p.value
+
+    def synchronize(self) -> None:
+        self._check(self._lib.c8r_synchronize(self._h))

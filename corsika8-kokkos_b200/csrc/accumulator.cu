@@ -1,0 +1,889 @@
+// accumulator.cu — host side of libc8radio.so: the RadioAccumulator semantics
+// of corsika/detail/kokkos/radio/RadioAccumulator.inl over the sm_100a
+// kernels, and the extern "C" entry points declared in include/c8radio.h.
+//
+// Exceptions carry the reference's classes (std::invalid_argument,
+// std::logic_error, std::out_of_range, std::runtime_error, ...) and are
+// mapped to C8R_* status codes at the C boundary.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <mutex>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/c8radio.h"
+#include "radio_kernels.cuh"
+
+namespace c8r {
+namespace {
+
+constexpr std::size_t kDefaultHostBatch = 4096;   // RadioAccumulator.hpp:49
+constexpr std::size_t kDirectThreshold = 16384;   // RadioAccumulator.hpp:101
+
+struct cuda_error : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+void check(cudaError_t err, char const* what) {
+  if (err != cudaSuccess)
+    throw cuda_error(std::string(what) + ": " + cudaGetErrorString(err));
+}
+
+template <class T>
+struct DeviceBuffer {
+  T* ptr = nullptr;
+  std::size_t count = 0;
+  DeviceBuffer() = default;
+  DeviceBuffer(DeviceBuffer const&) = delete;
+  DeviceBuffer& operator=(DeviceBuffer const&) = delete;
+  ~DeviceBuffer() { release(); }
+  void allocate(std::size_t n) {
+    release();
+    if (n == 0) return;
+    if (cudaMalloc(reinterpret_cast<void**>(&ptr), n * sizeof(T)) != cudaSuccess) {
+      ptr = nullptr;
+      cudaGetLastError();
+      throw std::bad_alloc();
+    }
+    count = n;
+  }
+  void release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    count = 0;
+  }
+  std::size_t bytes() const { return count * sizeof(T); }
+};
+
+template <class T>
+struct PinnedBuffer {
+  T* ptr = nullptr;
+  std::size_t count = 0;
+  PinnedBuffer() = default;
+  PinnedBuffer(PinnedBuffer const&) = delete;
+  PinnedBuffer& operator=(PinnedBuffer const&) = delete;
+  ~PinnedBuffer() {
+    if (ptr) cudaFreeHost(ptr);
+  }
+  void allocate(std::size_t n) {
+    if (ptr) cudaFreeHost(ptr);
+    ptr = nullptr;
+    count = 0;
+    if (n == 0) return;
+    if (cudaMallocHost(reinterpret_cast<void**>(&ptr), n * sizeof(T)) != cudaSuccess) {
+      ptr = nullptr;
+      cudaGetLastError();
+      throw std::bad_alloc();
+    }
+    count = n;
+  }
+};
+
+std::size_t checked_add(std::size_t a, std::size_t b) {
+  if (b > std::numeric_limits<std::size_t>::max() - a)
+    throw std::overflow_error("radio memory projection overflow");
+  return a + b;
+}
+std::size_t checked_mul(std::size_t a, std::size_t b) {
+  if (a != 0 && b > std::numeric_limits<std::size_t>::max() / a)
+    throw std::overflow_error("radio memory projection overflow");
+  return a * b;
+}
+
+// RadioAccumulator::validate, RadioAccumulator.inl:931-974.
+void validate(c8r_config const& config) {
+  auto const& p = config.propagation;
+  if (!config.coreas_enabled && !config.zhs_enabled)
+    throw std::invalid_argument("enabled radio has no algorithm");
+  if (!std::isfinite(config.fixed_point_field_limit_v_per_m) ||
+      !(config.fixed_point_field_limit_v_per_m > 0.))
+    throw std::invalid_argument("invalid radio fixed-point limit");
+  if (config.zhs_subtrack_refinement < 1 || config.zhs_subtrack_refinement > 64)
+    throw std::invalid_argument("ZHS subtrack refinement must be in [1,64]");
+  if (!std::isfinite(p.homogeneous_refractive_index) || p.homogeneous_refractive_index < 0.)
+    throw std::invalid_argument("invalid homogeneous radio refractive index");
+  bool const homogeneous = p.homogeneous_refractive_index > 0.;
+  if (!homogeneous &&
+      (p.table_size < 11 || p.refractivity == nullptr || p.integrated_refractivity == nullptr ||
+       !std::isfinite(p.minimum_height_m) || !std::isfinite(p.maximum_height_m) ||
+       !(p.maximum_height_m > p.minimum_height_m) || !std::isfinite(p.step_m) ||
+       !(p.step_m > 0.) || !std::isfinite(p.inverse_step_per_m) ||
+       !(p.inverse_step_per_m > 0.)))
+    throw std::invalid_argument("invalid flat-atmosphere radio snapshot");
+  if (config.precision != C8R_PRECISION_FP64 && config.precision != C8R_PRECISION_MIXED)
+    throw std::invalid_argument("invalid radio precision");
+  if (config.kernel < C8R_KERNEL_AUTO || config.kernel > C8R_KERNEL_WINDOWED)
+    throw std::invalid_argument("invalid radio kernel selection");
+  auto check_observers = [&](c8r_observer_snapshot const* observers, uint64_t count) {
+    if (count != 0 && observers == nullptr) throw std::invalid_argument("null radio observers");
+    for (uint64_t i = 0; i < count; ++i) {
+      auto const& o = observers[i];
+      if (!std::isfinite(o.start_time_s) || !std::isfinite(o.duration_s) ||
+          !(o.duration_s >= 0.) || !std::isfinite(o.sample_rate_hz) || !(o.sample_rate_hz > 0.) ||
+          o.number_of_bins == 0)
+        throw std::invalid_argument("invalid radio observer");
+      double const height = (o.position_m[2] - p.minimum_height_m) * p.inverse_step_per_m;
+      if (!homogeneous && (!std::isfinite(height) || height < 0. ||
+                           height + 0.5 >= static_cast<double>(p.table_size)))
+        throw std::invalid_argument("radio observer outside propagation table");
+      for (double coordinate : o.position_m)
+        if (!std::isfinite(coordinate))
+          throw std::invalid_argument("radio observer position is not finite");
+    }
+  };
+  check_observers(config.coreas_observers, config.coreas_observer_count);
+  check_observers(config.zhs_observers, config.zhs_observer_count);
+}
+
+std::size_t total_bins(c8r_observer_snapshot const* observers, uint64_t count) {
+  std::size_t bins = 0;
+  for (uint64_t i = 0; i < count; ++i) {
+    if (observers[i].number_of_bins > std::numeric_limits<std::size_t>::max() - bins)
+      throw std::overflow_error("radio waveform bin overflow");
+    bins += static_cast<std::size_t>(observers[i].number_of_bins);
+  }
+  return bins;
+}
+
+}  // namespace
+
+// RadioAccumulator::projectedDeviceBytes, RadioAccumulator.inl:87-141 (for
+// this implementation's allocations).
+std::size_t projected_device_bytes(c8r_config const& config) {
+  if (!config.enabled) return 0;
+  validate(config);
+  bool const homogeneous = config.propagation.homogeneous_refractive_index > 0.;
+  std::size_t total = homogeneous ? 0 : checked_mul(config.propagation.table_size, 2 * sizeof(double));
+  std::size_t const nc = config.coreas_enabled ? config.coreas_observer_count : 0;
+  std::size_t const nz = config.zhs_enabled ? config.zhs_observer_count : 0;
+  total = checked_add(total, checked_mul(nc + nz, sizeof(ObserverCache)));
+  for (int a = 0; a < 2; ++a) {
+    auto const bins = a == 0 ? total_bins(config.coreas_observers, nc)
+                             : total_bins(config.zhs_observers, nz);
+    auto const values = checked_mul(bins, 3);
+    total = checked_add(total, checked_mul(values, sizeof(long long)));
+    total = checked_add(total, checked_mul(values, sizeof(double)));  // decode buffer
+  }
+  total = checked_add(total, sizeof(DeviceCounters) + sizeof(unsigned long long) + sizeof(unsigned));
+  total = checked_add(total, checked_mul(kDefaultHostBatch, sizeof(c8r_lepton_transport_record)));
+  return total;
+}
+
+class Accumulator {
+ public:
+  Accumulator(c8r_config const& config, c8r_tuning const& tuning, cudaStream_t stream)
+      : stream_(stream) {
+    if (tuning.team_size > static_cast<uint64_t>(kWindowThreads) ||
+        (tuning.team_size != 0 && tuning.team_size % 32 != 0))
+      throw std::invalid_argument("radio tuning is invalid");
+    enabled_ = config.enabled != 0;
+    tuning_ = tuning;
+    if (!enabled_) return;
+    validate(config);
+    check(cudaGetDevice(&device_), "cudaGetDevice");
+    check(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, device_), "SM count");
+    copy_config(config);
+    fixed_ = config.deterministic != 0;
+    precision_ = config.precision == C8R_PRECISION_MIXED ? Precision::kMixed : Precision::kFP64;
+    kernel_ = config.kernel;
+    host_batch_ = tuning.batch_size ? static_cast<std::size_t>(tuning.batch_size) : kDefaultHostBatch;
+    threads_ = tuning.team_size ? static_cast<int>(tuning.team_size) : 384;
+    upload_static();
+    allocate_traces();
+    counters_.allocate(1);
+    slot_.allocate(1);
+    next_item_.allocate(1);
+    staging_.allocate(host_batch_);
+    for (auto& h : host_) h.allocate(host_batch_);
+    for (auto& e : host_ready_) check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+    check(cudaEventCreate(&kernel_begin_), "event");
+    check(cudaEventCreate(&kernel_end_), "event");
+    fuse_ = coreas_enabled_ && zhs_enabled_ && observers_share_grid();
+    initialized_ = true;
+    reset();
+  }
+
+  ~Accumulator() {
+    if (stream_ || initialized_) cudaStreamSynchronize(stream_);
+    for (auto& e : host_ready_)
+      if (e) cudaEventDestroy(e);
+    if (kernel_begin_) cudaEventDestroy(kernel_begin_);
+    if (kernel_end_) cudaEventDestroy(kernel_end_);
+  }
+
+  bool enabled() const { return initialized_ && enabled_; }
+
+  // RadioAccumulator::reset, RadioAccumulator.inl:224-250.
+  void reset() {
+    if (!enabled()) return;
+    if (host_count_ != 0) throw std::logic_error("cannot reset radio with uncommitted host tracks");
+    for (int a = 0; a < 2; ++a) {
+      if (fixed_traces_[a].ptr)
+        check(cudaMemsetAsync(fixed_traces_[a].ptr, 0, fixed_traces_[a].bytes(), stream_), "memset");
+      if (float_traces_[a].ptr)
+        check(cudaMemsetAsync(float_traces_[a].ptr, 0, float_traces_[a].bytes(), stream_), "memset");
+    }
+    check(cudaMemsetAsync(counters_.ptr, 0, sizeof(DeviceCounters), stream_), "memset");
+    check(cudaStreamSynchronize(stream_), "reset fence");
+    stats_ = c8r_statistics{};
+    stats_.device_bytes = device_bytes();
+    stats_.track_tile_size = static_cast<uint32_t>(chunk_hint());
+    stats_.observer_tile_size = static_cast<uint32_t>(window_bins_);
+    downloaded_ = false;
+    sealed_ = false;
+  }
+
+  // RadioAccumulator::enqueueHostLeptonTracks, RadioAccumulator.inl:252-272.
+  void enqueue_host(c8r_lepton_transport_record const* records, std::size_t count) {
+    if (!enabled()) throw std::logic_error("host radio tracks requested while radio is disabled");
+    if (downloaded_ || sealed_) throw std::logic_error("radio already downloaded; reset before host tracks");
+    if (count != 0 && records == nullptr) throw std::invalid_argument("null host radio track input");
+    while (count != 0) {
+      if (host_count_ == 0) check(cudaEventSynchronize(host_ready_[host_index_]), "staging wait");
+      std::size_t const copied = std::min(count, host_batch_ - host_count_);
+      std::memcpy(host_[host_index_].ptr + host_count_, records, copied * sizeof(*records));
+      host_count_ += copied;
+      stats_.host_tracks_enqueued += copied;
+      records += copied;
+      count -= copied;
+      if (host_count_ == host_batch_) flush();
+    }
+  }
+
+  // RadioAccumulator::flushHostLeptonTracks, RadioAccumulator.inl:274-290.  The
+  // staging half just filled is copied asynchronously; the other half can be
+  // filled while it uploads (double buffering replaces the reference's fence).
+  void flush() {
+    if (host_count_ == 0) return;
+    std::size_t const n = host_count_;
+    check(cudaMemcpyAsync(staging_.ptr, host_[host_index_].ptr, n * sizeof(c8r_lepton_transport_record),
+                          cudaMemcpyHostToDevice, stream_),
+          "host track upload");
+    check(cudaEventRecord(host_ready_[host_index_], stream_), "event");
+    host_index_ ^= 1;
+    host_count_ = 0;
+    accumulate_device(staging_.ptr, n, staging_.count);
+    stats_.host_to_device_bytes += n * sizeof(c8r_lepton_transport_record);
+    ++stats_.host_track_batches;
+  }
+
+  // RadioAccumulator::accumulateLeptonTracks, RadioAccumulator.inl:292-357.
+  void accumulate_device(c8r_lepton_transport_record const* records, std::size_t count,
+                         std::size_t extent) {
+    if (!enabled() || count == 0) return;
+    if (sealed_) throw std::logic_error("radio endpoint already committed; reset before new tracks");
+    if (count > extent) throw std::out_of_range("radio track count exceeds input view");
+    if (records == nullptr) throw std::invalid_argument("null device radio track input");
+    ensure_capacity(count);
+    check(cudaMemsetAsync(slot_.ptr, 0, sizeof(unsigned long long), stream_), "memset");
+    check(launch_ingest(records, count, tracks_.ptr, capacity_, slot_.ptr, counters_.ptr,
+                        diagnostics_, stream_),
+          "ingest launch");
+    ++stats_.track_precompute_batches;
+    stats_.track_precomputed_records += count;
+    stats_.maximum_track_batch = std::max<uint64_t>(stats_.maximum_track_batch, count);
+    if (timing_) check(cudaEventRecord(kernel_begin_, stream_), "event");
+    bool const direct = kernel_ == C8R_KERNEL_DIRECT ||
+                        (kernel_ == C8R_KERNEL_AUTO && count < kDirectThreshold);
+    if (direct)
+      project_direct(count);
+    else
+      project_windowed(count);
+    if (timing_) {
+      check(cudaEventRecord(kernel_end_, stream_), "event");
+      check(cudaEventSynchronize(kernel_end_), "event");
+      float ms = 0.f;
+      check(cudaEventElapsedTime(&ms, kernel_begin_, kernel_end_), "event time");
+      stats_.kernel_time_ms += ms;
+    }
+    downloaded_ = false;
+  }
+
+  // RadioAccumulator::download, RadioAccumulator.inl:407-439 (decode on the device).
+  void download(double* coreas, double* zhs, c8r_counters* counters) {
+    if (!enabled()) {
+      if (counters) *counters = c8r_counters{};
+      return;
+    }
+    if (downloaded_ || sealed_) throw std::logic_error("radio waveforms downloaded twice");
+    flush();
+    DeviceCounters host{};
+    fetch_counters(host);
+    if (host.fixed_point_overflows != 0)
+      throw std::runtime_error(
+          "radio fixed-point accumulator overflowed; increase fixed_point_field_limit_V_per_m");
+    for (int a = 0; a < 2; ++a) {
+      double* out = a == 0 ? coreas : zhs;
+      std::size_t const values = 3 * bins_[a];
+      if (values == 0 || out == nullptr) continue;
+      if (fixed_) {
+        check(launch_decode(reinterpret_cast<long long const*>(fixed_traces_[a].ptr), decoded_[a].ptr,
+                            bins_[a], decode_offsets_[a].ptr, decode_factors_[a].ptr,
+                            static_cast<uint32_t>(observers_host_[a].size()), max_observer_bins_[a],
+                            stream_),
+              "decode launch");
+        check(cudaMemcpyAsync(out, decoded_[a].ptr, values * sizeof(double), cudaMemcpyDeviceToHost,
+                              stream_),
+              "trace download");
+      } else {
+        check(cudaMemcpyAsync(out, float_traces_[a].ptr, values * sizeof(double),
+                              cudaMemcpyDeviceToHost, stream_),
+              "trace download");
+      }
+      stats_.device_to_host_bytes += values * sizeof(double);
+    }
+    check(cudaStreamSynchronize(stream_), "download fence");
+    if (counters) std::memcpy(counters, &host, sizeof(host));
+    downloaded_ = true;
+  }
+
+  // RadioAccumulator::downloadFixed, RadioAccumulator.inl:359-405: raw int64.
+  void download_fixed(long long* coreas, long long* zhs, c8r_counters* counters) {
+    if (!enabled() || !fixed_ || downloaded_ || sealed_)
+      throw std::logic_error("fixed radio snapshot unavailable/already committed");
+    flush();
+    sealed_ = true;
+    DeviceCounters host{};
+    fetch_counters(host);
+    for (int a = 0; a < 2; ++a) {
+      long long* out = a == 0 ? coreas : zhs;
+      std::size_t const values = 3 * bins_[a];
+      if (values == 0 || out == nullptr) continue;
+      check(cudaMemcpyAsync(out, fixed_traces_[a].ptr, values * sizeof(long long),
+                            cudaMemcpyDeviceToHost, stream_),
+            "fixed trace download");
+      stats_.device_to_host_bytes += values * sizeof(long long);
+    }
+    check(cudaStreamSynchronize(stream_), "download fence");
+    if (counters) std::memcpy(counters, &host, sizeof(host));
+    downloaded_ = true;
+  }
+
+  void statistics(c8r_statistics& out) const { out = stats_; }
+
+  std::size_t device_bytes() const {
+    std::size_t total = table_.bytes() + counters_.bytes() + slot_.bytes() + next_item_.bytes() +
+                        staging_.bytes() + tracks_.bytes();
+    for (int a = 0; a < 2; ++a)
+      total += observers_[a].bytes() + fixed_traces_[a].bytes() + float_traces_[a].bytes() +
+               decoded_[a].bytes() + decode_offsets_[a].bytes() + decode_factors_[a].bytes();
+    return total;
+  }
+
+  std::size_t static_host_to_device_bytes() const {
+    return table_.bytes() + observers_[0].bytes() + observers_[1].bytes();
+  }
+
+  // RadioAccumulator::reserveTrackCapacity / projectedTrackCapacity.
+  void reserve(std::size_t count) {
+    if (!enabled() || count == 0) return;
+    ensure_capacity(count);
+  }
+  void projected_track_capacity(std::size_t count, std::size_t& retained, std::size_t& peak) const {
+    std::size_t const current = device_bytes();
+    retained = peak = current;
+    if (!enabled() || count == 0 || count <= capacity_) return;
+    if (capacity_ > std::numeric_limits<std::size_t>::max() / 2)
+      throw std::length_error("radio track capacity overflow");
+    std::size_t const grown = capacity_ == 0 ? count : std::max(count, 2 * capacity_);
+    std::size_t const old_bytes = tracks_.bytes();
+    std::size_t const new_bytes = checked_mul(checked_mul(grown, kTrackRows), sizeof(double));
+    retained = current - old_bytes + new_bytes;
+    peak = checked_add(current, new_bytes);
+  }
+
+  void synchronize() { check(cudaStreamSynchronize(stream_), "stream synchronize"); }
+
+  std::size_t bins(int a) const { return bins_[a]; }
+  void set_timing(bool on) { timing_ = on; }
+
+  // Work-plan access for the batched launcher.
+  EventPlan event_plan(std::size_t count) const { return make_event(count); }
+  bool fixed() const { return fixed_; }
+  Precision precision() const { return precision_; }
+  int sms() const { return sms_; }
+  int threads() const { return threads_; }
+  uint32_t window_bins() const { return static_cast<uint32_t>(window_bins_); }
+
+ private:
+  void copy_config(c8r_config const& config) {
+    coreas_enabled_ = config.coreas_enabled != 0;
+    zhs_enabled_ = config.zhs_enabled != 0;
+    diagnostics_ = config.track_diagnostics != 0;
+    limit_ = config.fixed_point_field_limit_v_per_m;
+    deterministic_ = config.deterministic != 0;
+    auto const& p = config.propagation;
+    propagation_.homogeneous = p.homogeneous_refractive_index;
+    propagation_.min_height = p.minimum_height_m;
+    propagation_.max_height = p.maximum_height_m;
+    propagation_.step = p.step_m;
+    propagation_.inv_step = p.inverse_step_per_m;
+    propagation_.slope_n_lower = p.slope_refractivity_lower;
+    propagation_.slope_i_lower = p.slope_integrated_refractivity_lower;
+    propagation_.slope_n_upper = p.slope_refractivity_upper;
+    propagation_.slope_i_upper = p.slope_integrated_refractivity_upper;
+    propagation_.table_size = p.table_size;
+    propagation_.refinement = config.zhs_subtrack_refinement;
+    if (p.refractivity && p.integrated_refractivity && p.table_size) {
+      table_host_.resize(p.table_size);
+      for (std::size_t i = 0; i < p.table_size; ++i)
+        table_host_[i] = make_double2(p.refractivity[i], p.integrated_refractivity[i]);
+    }
+    if (coreas_enabled_)
+      snapshots_[0].assign(config.coreas_observers, config.coreas_observers + config.coreas_observer_count);
+    if (zhs_enabled_)
+      snapshots_[1].assign(config.zhs_observers, config.zhs_observers + config.zhs_observer_count);
+  }
+
+  // RadioAccumulator::makeObservers (RadioAccumulator.inl:522-550) plus the
+  // per-observer constants of propagate/add_sample, evaluated with the same
+  // IEEE operations the reference performs inline.
+  void make_observers(int a) {
+    auto& out = observers_host_[a];
+    out.clear();
+    std::size_t offset = 0;
+    bool const homogeneous = propagation_.homogeneous > 0.;
+    for (auto const& s : snapshots_[a]) {
+      ObserverCache o{};
+      o.px = s.position_m[0];
+      o.py = s.position_m[1];
+      o.pz = s.position_m[2];
+      o.start_time = s.start_time_s;
+      o.end_time = s.start_time_s + s.duration_s;
+      o.sample_rate = s.sample_rate_hz;
+      o.resolution = 1. / s.sample_rate_hz;
+      o.wavelength = kSpeedOfLight / s.sample_rate_hz;
+      double const factor = a == 1 ? s.sample_rate_hz : 1.;
+      o.fixed_scale = deterministic_ ? kHeadroom * factor / limit_ : 1.;
+      o.fixed_scale_f = static_cast<float>(o.fixed_scale);
+      o.bins_d = static_cast<double>(s.number_of_bins);
+      o.bins = s.number_of_bins;
+      o.offset = offset;
+      if (!homogeneous) {
+        o.dest_height = (s.position_m[2] - propagation_.min_height) * propagation_.inv_step;
+        o.dest_index = static_cast<uint64_t>(o.dest_height + 0.5);
+        o.dest_n = table_host_[o.dest_index].x + 1.;
+        o.dest_integral = table_host_[o.dest_index].y;
+      }
+      offset += static_cast<std::size_t>(s.number_of_bins);
+      out.push_back(o);
+    }
+    bins_[a] = offset;
+  }
+
+  bool observers_share_grid() const {
+    auto const& c = snapshots_[0];
+    auto const& z = snapshots_[1];
+    if (c.size() != z.size() || c.empty()) return false;
+    for (std::size_t i = 0; i < c.size(); ++i) {
+      if (c[i].start_time_s != z[i].start_time_s || c[i].duration_s != z[i].duration_s ||
+          c[i].sample_rate_hz != z[i].sample_rate_hz || c[i].number_of_bins != z[i].number_of_bins)
+        return false;
+      for (int axis = 0; axis < 3; ++axis)
+        if (c[i].position_m[axis] != z[i].position_m[axis]) return false;
+    }
+    return true;
+  }
+
+  void upload_static() {
+    if (!table_host_.empty() && propagation_.homogeneous <= 0.) {
+      table_.allocate(table_host_.size());
+      check(cudaMemcpy(table_.ptr, table_host_.data(), table_.bytes(), cudaMemcpyHostToDevice),
+            "table upload");
+    }
+    propagation_.table = table_.ptr;
+    std::size_t largest = 0;
+    for (int a = 0; a < 2; ++a) {
+      make_observers(a);
+      auto const& host = observers_host_[a];
+      if (!host.empty()) {
+        observers_[a].allocate(host.size());
+        check(cudaMemcpy(observers_[a].ptr, host.data(), observers_[a].bytes(), cudaMemcpyHostToDevice),
+              "observer upload");
+      }
+      max_observer_bins_[a] = 0;
+      std::vector<uint64_t> offsets;
+      std::vector<double> factors;
+      for (auto const& s : snapshots_[a]) {
+        max_observer_bins_[a] = std::max<uint64_t>(max_observer_bins_[a], s.number_of_bins);
+        // downloadSet's inverse scale, RadioAccumulator.inl:865-867
+        double const factor = a == 1 ? s.sample_rate_hz : 1.;
+        factors.push_back(limit_ / (kHeadroom * factor));
+      }
+      for (auto const& o : host) offsets.push_back(o.offset);
+      offsets.push_back(bins_[a]);
+      largest = std::max<std::size_t>(largest, max_observer_bins_[a]);
+      if (!host.empty()) {
+        decode_offsets_[a].allocate(offsets.size());
+        decode_factors_[a].allocate(factors.size());
+        check(cudaMemcpy(decode_offsets_[a].ptr, offsets.data(), decode_offsets_[a].bytes(),
+                         cudaMemcpyHostToDevice),
+              "decode upload");
+        check(cudaMemcpy(decode_factors_[a].ptr, factors.data(), decode_factors_[a].bytes(),
+                         cudaMemcpyHostToDevice),
+              "decode upload");
+      }
+    }
+    int const device_window = windowed_max_bins(device_);
+    std::size_t window = largest;
+    if (tuning_.observer_tile_size != 0) window = std::min<std::size_t>(window, tuning_.observer_tile_size);
+    window_bins_ = std::min<std::size_t>(window, static_cast<std::size_t>(device_window));
+    if (window_bins_ == 0) window_bins_ = 1;
+  }
+
+  void allocate_traces() {
+    for (int a = 0; a < 2; ++a) {
+      std::size_t const values = 3 * bins_[a];
+      if (values == 0) continue;
+      if (fixed_) {
+        fixed_traces_[a].allocate(values);
+        decoded_[a].allocate(values);
+      } else {
+        float_traces_[a].allocate(values);
+      }
+    }
+  }
+
+  void ensure_capacity(std::size_t count) {
+    if (capacity_ >= count) return;
+    if (capacity_ > std::numeric_limits<std::size_t>::max() / 2)
+      throw std::length_error("radio track capacity overflow");
+    std::size_t const grown = capacity_ == 0 ? count : std::max(count, 2 * capacity_);
+    if (capacity_ != 0) check(cudaStreamSynchronize(stream_), "grow fence");
+    tracks_.allocate(checked_mul(grown, kTrackRows));
+    capacity_ = grown;
+    stats_.track_workspace_bytes = tracks_.bytes();
+    stats_.device_bytes = device_bytes();
+  }
+
+  std::size_t chunk_hint() const { return tuning_.track_tile_size; }
+
+  EventPlan make_event(std::size_t count) const {
+    EventPlan ev{};
+    ev.tracks = tracks_.ptr;
+    ev.stride = capacity_;
+    ev.valid_tracks = slot_.ptr;
+    for (int a = 0; a < 2; ++a) {
+      bool const on = a == 0 ? coreas_enabled_ : zhs_enabled_;
+      ev.observers[a] = observers_[a].ptr;
+      ev.observer_count[a] = on ? static_cast<uint32_t>(observers_host_[a].size()) : 0;
+      ev.fixed[a] = fixed_traces_[a].ptr;
+      ev.floating[a] = float_traces_[a].ptr;
+      ev.total_bins[a] = bins_[a];
+    }
+    ev.propagation = propagation_;
+    ev.counters = counters_.ptr;
+    ev.window = static_cast<uint32_t>(window_bins_);
+    uint32_t const per_chunk = ev.observer_count[0] + ev.observer_count[1];
+    std::size_t chunk = tuning_.track_tile_size;
+    if (chunk == 0) {
+      // about 16 work items per persistent CTA, at least 8192 tracks each
+      std::size_t const ctas = static_cast<std::size_t>(sms_) * 2;
+      std::size_t const target_chunks = std::max<std::size_t>(1, (16 * ctas + per_chunk - 1) / std::max<uint32_t>(per_chunk, 1));
+      chunk = std::max<std::size_t>(8192, (count + target_chunks - 1) / target_chunks);
+    }
+    chunk = std::min<std::size_t>(chunk, 0x7fffffffu);
+    ev.chunk_size = static_cast<uint32_t>(chunk);
+    ev.chunks = static_cast<uint32_t>((count + chunk - 1) / chunk);
+    return ev;
+  }
+
+  void project_direct(std::size_t count) {
+    EventPlan const ev = make_event(count);
+    bool const c = ev.observer_count[0] != 0, z = ev.observer_count[1] != 0;
+    if (fuse_) {
+      check(launch_direct(ev, count, true, true, fixed_, precision_, stream_), "direct launch");
+    } else {
+      if (c) check(launch_direct(ev, count, true, false, fixed_, precision_, stream_), "direct launch");
+      if (z) check(launch_direct(ev, count, false, true, fixed_, precision_, stream_), "direct launch");
+    }
+    uint64_t const pairs_c = count * ev.observer_count[0], pairs_z = count * ev.observer_count[1];
+    stats_.track_observer_pairs += pairs_c + pairs_z;
+    if (fuse_) stats_.fused_track_observer_pairs += pairs_c;
+    ++stats_.direct_projection_batches;
+    stats_.direct_projection_records += count;
+  }
+
+  void project_windowed(std::size_t count) {
+    WorkPlan plan{};
+    plan.events[0] = make_event(count);
+    plan.events[0].first_item = 0;
+    uint32_t const per_chunk = plan.events[0].observer_count[0] + plan.events[0].observer_count[1];
+    plan.event_count = 1;
+    plan.window = plan.events[0].window;
+    plan.total_items = static_cast<uint64_t>(plan.events[0].chunks) * per_chunk;
+    plan.next_item = next_item_.ptr;
+    int per_sm = windowed_ctas_per_sm(static_cast<int>(plan.window), threads_, fixed_, precision_);
+    if (per_sm <= 0) throw cuda_error("windowed radio kernel does not fit on this device");
+    uint64_t ctas = static_cast<uint64_t>(per_sm) * sms_;
+    if (ctas > plan.total_items) ctas = plan.total_items;
+    check(cudaMemsetAsync(next_item_.ptr, 0, sizeof(unsigned), stream_), "memset");
+    check(launch_windowed(plan, fixed_, precision_, static_cast<int>(ctas), threads_, stream_),
+          "windowed launch");
+    uint64_t const pairs_c = count * plan.events[0].observer_count[0];
+    uint64_t const pairs_z = count * plan.events[0].observer_count[1];
+    stats_.track_observer_pairs += pairs_c + pairs_z;
+    if (fuse_) stats_.fused_track_observer_pairs += pairs_c;
+    stats_.projection_tiles += plan.total_items;
+  }
+
+  void fetch_counters(DeviceCounters& host) {
+    check(cudaMemcpyAsync(&host, counters_.ptr, sizeof(host), cudaMemcpyDeviceToHost, stream_),
+          "counter download");
+    check(cudaStreamSynchronize(stream_), "counter fence");
+    stats_.lepton_tracks = host.valid_tracks;
+    stats_.coreas_contributions = host.coreas_contributions;
+    stats_.zhs_contributions = host.zhs_contributions;
+    stats_.zhs_subtracks = host.zhs_subtracks;
+    stats_.fixed_point_overflows = host.fixed_point_overflows;
+    std::memcpy(&stats_.counters, &host, sizeof(host));
+    stats_.device_to_host_bytes += sizeof(host);
+  }
+
+  cudaStream_t stream_ = nullptr;
+  int device_ = 0;
+  int sms_ = 148;
+  int threads_ = 384;
+  bool enabled_ = false;
+  bool initialized_ = false;
+  bool coreas_enabled_ = false, zhs_enabled_ = false, diagnostics_ = false;
+  bool fixed_ = true, deterministic_ = true, fuse_ = false;
+  bool downloaded_ = false, sealed_ = false, timing_ = false;
+  int kernel_ = C8R_KERNEL_AUTO;
+  Precision precision_ = Precision::kFP64;
+  double limit_ = 1.;
+  c8r_tuning tuning_{};
+  Propagation propagation_{};
+  std::vector<double2> table_host_;
+  std::vector<c8r_observer_snapshot> snapshots_[2];
+  std::vector<ObserverCache> observers_host_[2];
+  std::size_t bins_[2] = {0, 0};
+  uint64_t max_observer_bins_[2] = {0, 0};
+  std::size_t window_bins_ = 0;
+  DeviceBuffer<double2> table_;
+  DeviceBuffer<ObserverCache> observers_[2];
+  DeviceBuffer<unsigned long long> fixed_traces_[2];
+  DeviceBuffer<double> float_traces_[2];
+  DeviceBuffer<double> decoded_[2];
+  DeviceBuffer<uint64_t> decode_offsets_[2];
+  DeviceBuffer<double> decode_factors_[2];
+  DeviceBuffer<DeviceCounters> counters_;
+  DeviceBuffer<unsigned long long> slot_;
+  DeviceBuffer<unsigned> next_item_;
+  DeviceBuffer<double> tracks_;
+  std::size_t capacity_ = 0;
+  DeviceBuffer<c8r_lepton_transport_record> staging_;
+  PinnedBuffer<c8r_lepton_transport_record> host_[2];
+  cudaEvent_t host_ready_[2] = {nullptr, nullptr};
+  cudaEvent_t kernel_begin_ = nullptr, kernel_end_ = nullptr;
+  int host_index_ = 0;
+  std::size_t host_count_ = 0;
+  std::size_t host_batch_ = kDefaultHostBatch;
+  c8r_statistics stats_{};
+};
+
+}  // namespace c8r
+
+// ============================================================== C boundary
+struct c8r_accumulator {
+  c8r::Accumulator* impl = nullptr;
+  std::string error;
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+template <class F>
+int guarded(std::string* error, F&& body) {
+  try {
+    body();
+    return C8R_OK;
+  } catch (std::invalid_argument const& e) {
+    if (error) *error = e.what();
+    return C8R_INVALID_ARGUMENT;
+  } catch (std::out_of_range const& e) {
+    if (error) *error = e.what();
+    return C8R_OUT_OF_RANGE;
+  } catch (std::length_error const& e) {
+    if (error) *error = e.what();
+    return C8R_LENGTH_ERROR;
+  } catch (std::logic_error const& e) {
+    if (error) *error = e.what();
+    return C8R_LOGIC_ERROR;
+  } catch (std::overflow_error const& e) {
+    if (error) *error = e.what();
+    return C8R_OVERFLOW_ERROR;
+  } catch (c8r::cuda_error const& e) {
+    if (error) *error = e.what();
+    return C8R_CUDA_ERROR;
+  } catch (std::runtime_error const& e) {
+    if (error) *error = e.what();
+    return C8R_RUNTIME_ERROR;
+  } catch (std::bad_alloc const&) {
+    if (error) *error = "radio allocation failed";
+    return C8R_BAD_ALLOC;
+  } catch (...) {
+    if (error) *error = "unknown radio failure";
+    return C8R_RUNTIME_ERROR;
+  }
+}
+
+int with_handle(c8r_accumulator const* h, std::string* error_slot, bool need) {
+  (void)error_slot;
+  if (h == nullptr || (need && h->impl == nullptr)) {
+    g_last_error = "null radio accumulator handle";
+    return C8R_INVALID_ARGUMENT;
+  }
+  return C8R_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* c8r_version(void) { return "c8radio-b200 1.0 (sm_100a)"; }
+
+const char* c8r_last_error(const c8r_accumulator* handle) {
+  if (handle == nullptr) return g_last_error.c_str();
+  return handle->error.c_str();
+}
+
+const char* c8r_last_global_error(void) { return g_last_error.c_str(); }
+
+int c8r_config_validate(const c8r_config* config) {
+  return guarded(&g_last_error, [&] {
+    if (!config) throw std::invalid_argument("null radio config");
+    c8r::validate(*config);
+  });
+}
+
+int c8r_projected_device_bytes(const c8r_config* config, size_t* bytes) {
+  return guarded(&g_last_error, [&] {
+    if (!config || !bytes) throw std::invalid_argument("null argument");
+    *bytes = c8r::projected_device_bytes(*config);
+  });
+}
+
+int c8r_create(const c8r_config* config, const c8r_tuning* tuning, void* stream,
+               c8r_accumulator** handle) {
+  return guarded(&g_last_error, [&] {
+    if (!config || !handle) throw std::invalid_argument("null argument");
+    *handle = nullptr;
+    c8r_tuning const t = tuning ? *tuning : c8r_tuning{};
+    auto* h = new c8r_accumulator;
+    try {
+      h->impl = new c8r::Accumulator(*config, t, static_cast<cudaStream_t>(stream));
+    } catch (...) {
+      delete h;
+      throw;
+    }
+    *handle = h;
+  });
+}
+
+void c8r_destroy(c8r_accumulator* handle) {
+  if (!handle) return;
+  delete handle->impl;
+  delete handle;
+}
+
+int c8r_enabled(const c8r_accumulator* handle, int* enabled) {
+  if (int s = with_handle(handle, nullptr, true)) return s;
+  if (!enabled) return C8R_INVALID_ARGUMENT;
+  *enabled = handle->impl->enabled() ? 1 : 0;
+  return C8R_OK;
+}
+
+int c8r_reset(c8r_accumulator* handle) {
+  if (int s = with_handle(handle, nullptr, true)) return s;
+  return guarded(&handle->error, [&] { handle->impl->reset(); });
+}
+
+int c8r_enqueue_host(c8r_accumulator* handle, const c8r_lepton_transport_record* records,
+                     size_t count) {
+  if (int s = with_handle(handle, nullptr, true)) return s;
+  return guarded(&handle->error, [&] { handle->impl->enqueue_host(records, count); });
+}
+
+int c8r_flush(c8r_accumulator* handle) {
+  if (int s = with_handle(handle, nullptr, true)) return s;
+  return guarded(&handle->error, [&] { handle->impl->flush(); });
+}
+
+int c8r_accumulate_device(c8r_accumulator* handle, const c8r_lepton_transport_record* records,
+                          size_t count, size_t extent) {
+  if (int s = with_handle(handle, nullptr, true)) return s;
+  return guarded(&handle->error,
+                 [&] { handle->impl->accumulate_device(records, count, extent); });
+}
+
+int c8r_download(c8r_accumulator* handle, double* coreas_xyz, double* zhs_xyz,
+                 c8r_counters* counters) {
+  if (int s = with_handle(handle, nullptr, true)) return s;
+  return guarded(&handle->error, [&] { handle->impl->download(coreas_xyz, zhs_xyz, counters); });
+}
+
+int c8r_download_fixed(c8r_accumulator* handle, long long* coreas_xyz, long long* zhs_xyz,
+                       c8r_counters* counters) {
+  if (int s = with_handle(handle, nullptr, true)) return s;
+  return guarded(&handle->error,
+                 [&] { handle->impl->download_fixed(coreas_xyz, zhs_xyz, counters); });
+}
+
+int c8r_total_bins(const c8r_accumulator* handle, size_t* coreas_bins, size_t* zhs_bins) {
+  if (int s = with_handle(handle, nullptr, true)) return s;
+  if (coreas_bins) *coreas_bins = handle->impl->bins(0);
+  if (zhs_bins) *zhs_bins = handle->impl->bins(1);
+  return C8R_OK;
+}
+
+int c8r_get_statistics(const c8r_accumulator* handle, c8r_statistics* statistics) {
+  if (int s = with_handle(handle, nullptr, true)) return s;
+  if (!statistics) return C8R_INVALID_ARGUMENT;
+  handle->impl->statistics(*statistics);
+  return C8R_OK;
+}
+
+int c8r_device_bytes(const c8r_accumulator* handle, size_t* bytes) {
+  if (int s = with_handle(handle, nullptr, true)) return s;
+  if (!bytes) return C8R_INVALID_ARGUMENT;
+  *bytes = handle->impl->device_bytes();
+  return C8R_OK;
+}
+
+int c8r_static_host_to_device_bytes(const c8r_accumulator* handle, size_t* bytes) {
+  if (int s = with_handle(handle, nullptr, true)) return s;
+  if (!bytes) return C8R_INVALID_ARGUMENT;
+  *bytes = handle->impl->static_host_to_device_bytes();
+  return C8R_OK;
+}
+
+int c8r_reserve(c8r_accumulator* handle, size_t count) {
+  if (int s = with_handle(handle, nullptr, true)) return s;
+  return guarded(&handle->error, [&] { handle->impl->reserve(count); });
+}
+
+int c8r_projected_track_capacity(const c8r_accumulator* handle, size_t count,
+                                 size_t* retained_bytes, size_t* transient_peak_bytes) {
+  if (int s = with_handle(handle, nullptr, true)) return s;
+  std::size_t r = 0, p = 0;
+  int const status = guarded(const_cast<std::string*>(&handle->error),
+                             [&] { handle->impl->projected_track_capacity(count, r, p); });
+  if (retained_bytes) *retained_bytes = r;
+  if (transient_peak_bytes) *transient_peak_bytes = p;
+  return status;
+}
+
+int c8r_synchronize(c8r_accumulator* handle) {
+  if (int s = with_handle(handle, nullptr, true)) return s;
+  return guarded(&handle->error, [&] { handle->impl->synchronize(); });
+}
+
+}  // extern "C"

@@ -1,0 +1,213 @@
+// radio_device.cuh — device arithmetic of the radio projection (sm_100a).
+//
+// Every FP64 expression that decides a time bin, a branch or (in the FP64
+// path) an amplitude is written with the reference's association order
+// (corsika/detail/kokkos/radio/algorithms/RadioProjection.inl) and this file
+// is compiled with -fmad=false, so no multiply-add is contracted: results are
+// the IEEE-754 results the x86-64 host produces for the same source.
+// Amplitudes take the type `Amp`: double for the FP64 drop-in, float for the
+// mixed-precision path.
+#pragma once
+
+#include <cstdint>
+#include <climits>
+
+namespace c8r {
+
+// corsika/kokkos/ScalarPhysicalConstants.hpp:18-20, RadioProjectionData.hpp:21-37
+constexpr double kSpeedOfLight = 299792458.;
+constexpr double kElementaryCharge = 1.6021766208e-19;
+constexpr double kVacuumPermittivity = 8.8541878128e-12;
+constexpr double kPi = 3.141592653589793238462643383279502884;
+constexpr double kCoreasThreshold = 1.e-3;
+constexpr double kHeadroom = 4611686018427387904.0;     // 2^62
+constexpr double kSignedLimit = 9223372036854775808.0;  // 2^63
+constexpr double kElectronMassGeV = 5.109989e-4;        // TransportMass.hpp:20
+
+// Per-observer constants, derived on the host with the same IEEE operations
+// the reference evaluates inline (destination bin of propagate, window end of
+// add_sample, grid resolution and wavelength).
+struct alignas(16) ObserverCache {
+  double px, py, pz;
+  double start_time;     // startTimeS_
+  double end_time;       // startTimeS_ + durationS_   (RadioProjection.inl:273)
+  double sample_rate;    // sampleRateHz_
+  double resolution;     // 1. / sampleRateHz_         (:374, :396)
+  double wavelength;     // c / sampleRateHz_          (:492)
+  double fixed_scale;    // fixedPointScale_
+  double bins_d;         // (double) numberOfBins_     (:280)
+  uint64_t bins;
+  uint64_t offset;       // waveformOffset_
+  double dest_height;    // (z - minimumHeightM_) * inverseStepPerM_   (:184-185)
+  double dest_n;         // refractivity_[dest] + 1.                   (:191)
+  double dest_integral;  // integratedRefractivity_[dest]              (:192)
+  uint64_t dest_index;   // static_cast<size_t>(dest_height + 0.5)      (:187)
+  float fixed_scale_f;
+  uint32_t pad_;
+};
+
+// RadioPropagationView with the two tables interleaved as {n-1, integral}.
+struct Propagation {
+  double homogeneous;
+  double min_height;
+  double max_height;
+  double step;
+  double inv_step;
+  double slope_n_lower;
+  double slope_i_lower;
+  double slope_n_upper;
+  double slope_i_upper;
+  const double2* table;  // .x = refractivity, .y = integrated refractivity
+  uint64_t table_size;
+  uint32_t refinement;
+  uint32_t pad_;
+};
+
+// Track kinematics in registers (RadioTrackKinematics minus derived vectors).
+struct Track {
+  double sx, sy, sz, ex, ey, ez;
+  double ts, te;
+  double bx, by, bz;
+  double length, beta_module, constant;
+};
+
+// Structure-of-arrays track workspace: 14 rows of `capacity` doubles.
+enum TrackRow : int {
+  kSx = 0, kSy, kSz, kEx, kEy, kEz, kTs, kTe, kBx, kBy, kBz, kLen, kBmod, kConst, kTrackRows
+};
+
+struct Path {
+  double time, n_src, n_dst, dist, kx, ky, kz;
+};
+
+// static_cast<int>(double) as x86-64 executes it (cvttsd2si): out of range and
+// NaN give INT_MIN.  The reference's host build relies on it for ZHS bin spans
+// and subtrack counts (RadioProjection.inl:457, :502).
+__device__ __forceinline__ int x86_int(double v) {
+  if (!(v > -2147483649.0 && v < 2147483648.0)) return INT_MIN;
+  return static_cast<int>(v);
+}
+
+// static_cast<long long>(double) as x86-64 executes it (cvttsd2si, 64-bit).
+__device__ __forceinline__ long long x86_ll(double v) {
+  if (!(v >= -9223372036854775808.0 && v < 9223372036854775808.0)) return LLONG_MIN;
+  return static_cast<long long>(v);
+}
+
+// observer_nearest_bin, RadioProjection.inl:75-82.
+__device__ __forceinline__ double nearest_bin(double scaled) {
+  double const integral = floor(scaled);
+  return integral + (scaled - integral >= 0.5 ? 1. : 0.);
+}
+
+// co_reas_doppler, RadioProjection.inl:113-143 (device branch).
+__device__ __forceinline__ double doppler(double index, double bx, double by, double bz,
+                                          double kx, double ky, double kz) {
+  double const ordinary = 1. - index * (bx * kx + by * ky + bz * kz);
+  if (ordinary != 0.) return ordinary;
+  double const px = bx * kx, py = by * ky, pz = bz * kz;
+  double const ex = fma(bx, kx, -px), ey = fma(by, ky, -py), ez = fma(bz, kz, -pz);
+  double const xy = px + py;
+  double const xy_virtual = xy - px;
+  double const xy_error = (px - (xy - xy_virtual)) + (py - xy_virtual);
+  double const xyz = xy + pz;
+  double const xyz_virtual = xyz - xy;
+  double const xyz_error = (xy - (xyz - xyz_virtual)) + (pz - xyz_virtual);
+  double const low = ex + ey + ez + xy_error + xyz_error;
+  double const product = index * xyz;
+  double const product_error = fma(index, xyz, -product) + index * low;
+  return (1. - product) - product_error;
+}
+
+// propagate, RadioProjection.inl:170-238.  kTime = false skips the refractive
+// index and travel time (the Fraunhofer midpoint uses only k and distance).
+template <bool kTime>
+__device__ __forceinline__ Path propagate(Propagation const& p, ObserverCache const& o,
+                                          double sx, double sy, double sz) {
+  Path r;
+  double const dx = o.px - sx, dy = o.py - sy, dz = o.pz - sz;
+  double const dist = sqrt(dx * dx + dy * dy + dz * dz);
+  r.kx = dx / dist;
+  r.ky = dy / dist;
+  r.kz = dz / dist;
+  r.dist = dist;
+  if (!kTime) return r;
+  if (p.homogeneous > 0.) {
+    r.time = p.homogeneous * dist / kSpeedOfLight;
+    r.n_src = r.n_dst = p.homogeneous;
+    return r;
+  }
+  double const sh = (sz - p.min_height) * p.inv_step;
+  double const dh = o.dest_height;
+  uint64_t const last = p.table_size - 1;
+  double n_src = 1., i_src = 1., n_dst = o.dest_n, height = 1.;
+  if (sh + 0.5 >= static_cast<double>(last)) {
+    double2 const t = __ldg(p.table + last);
+    n_src = t.x + p.slope_n_upper * fabs((sz - p.max_height) * p.inv_step) + 1.;
+    i_src = t.y + p.slope_i_upper * fabs(p.max_height - sz);
+    height = sh - dh;
+  } else if (sh + 0.5 < static_cast<double>(last) && sh > 0.) {
+    uint64_t const si = static_cast<uint64_t>(sh + 0.5);
+    double2 const t = __ldg(p.table + si);
+    n_src = t.x + 1.;
+    i_src = t.y;
+    height = static_cast<double>(static_cast<int64_t>(si) - static_cast<int64_t>(o.dest_index)) *
+             p.step;
+    if (height == 0.) height = 1.;
+  } else if (sh == 0.) {
+    n_src = 1.;
+    n_dst = 1.;
+    i_src = __ldg(p.table).y;
+    height = dh - sh;
+  } else {
+    double2 const t0 = __ldg(p.table);
+    n_src = t0.x + p.slope_n_lower * fabs(sh) + 1.;
+    i_src = t0.y + p.slope_i_lower * fabs(sh);
+    n_dst = 1.;
+    height = dh - fabs(sh);
+  }
+  r.time = (1. + (i_src - o.dest_integral) / height) * dist / kSpeedOfLight;
+  r.n_src = n_src;
+  r.n_dst = n_dst;
+  return r;
+}
+
+// separate_same_bin_endpoints, RadioProjection.inl:303-336.
+__device__ __forceinline__ void separate_same_bin(double& start, double& end, double res,
+                                                  bool signed_order) {
+  long long const sb = x86_ll(nearest_bin(start / res));
+  long long const eb = x86_ll(nearest_bin(end / res));
+  if (sb != eb) return;
+  double const sf = start / res - floor(start / res);
+  double const ef = end / res - floor(end / res);
+  bool const forward = !signed_order || end >= start;
+  if (forward) {
+    if (sf >= 0.5 && ef >= 0.5) start -= res;
+    else if (sf < 0.5 && ef < 0.5) end += res;
+    else if (ef >= 1. - sf) end += res;
+    else start -= res;
+  } else {
+    if (sf >= 0.5 && ef >= 0.5) end -= res;
+    else if (sf < 0.5 && ef < 0.5) start += res;
+    else if (sf >= 1. - ef) start += res;
+    else end -= res;
+  }
+}
+
+template <class T>
+struct Vec3 {
+  T x, y, z;
+};
+
+// k x (k x beta) (transverse_endpoint, :240-243) and k x (beta x k) (:438).
+template <class T>
+__device__ __forceinline__ Vec3<T> cross(Vec3<T> a, Vec3<T> b) {
+  return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+
+// Per-thread event counters (RadioCounters' projection fields).
+struct Counts {
+  unsigned long long coreas = 0, zhs = 0, subtracks = 0, overflows = 0;
+};
+
+}  // namespace c8r

@@ -1,0 +1,811 @@
+// radio_kernels.cu — sm_100a kernels of the radio projection.
+//
+// Compiled with -fmad=false (see build.py): FP64 time/bin/branch arithmetic is
+// the IEEE result of the reference's expressions, so fixed-point traces in the
+// FP64 path are bit-identical to the reference's, and bin indices and branch
+// decisions are identical in the mixed path too.
+//
+//   ingest_kernel    LeptonTransportRecord (752 B AoS) -> compacted SoA
+//                    kinematics + counters (record_track, RadioProjection.inl:541-611)
+//   direct_kernel    one thread per (track, antenna) pair, 64-bit global
+//                    atomics per sample (RadioAccumulator.inl:663-697 shape)
+//   windowed_kernel  persistent CTAs over a work list of (event, chunk,
+//                    algorithm, antenna) items; the CTA owns that antenna's
+//                    trace as an int64 window in shared memory, deposits with
+//                    shared atomics and flushes non-zero bins with checked
+//                    global atomics
+//   decode_kernel    int64 fixed point -> V/m (V s/m) (RadioAccumulator.inl:849-898)
+#include "radio_kernels.cuh"
+
+#include <cuda_runtime.h>
+
+#include "../../include/c8radio.h"
+
+namespace c8r {
+namespace {
+
+constexpr double kEmConstant = 1. / (4. * kPi * kVacuumPermittivity * kSpeedOfLight);
+
+// ---------------------------------------------------------------- fixed point
+// add_radio_fixed_point, RadioProjection.inl:254-260.
+__device__ __forceinline__ bool to_fixed(double v, ObserverCache const& o, long long& out) {
+  double const s = v * o.fixed_scale;
+  if (!isfinite(s) || fabs(s) >= kSignedLimit) return false;
+  out = __double2ll_rn(s);
+  return true;
+}
+__device__ __forceinline__ bool to_fixed(float v, ObserverCache const& o, long long& out) {
+  float const s = v * o.fixed_scale_f;
+  if (!isfinite(s) || fabsf(s) >= 9223372036854775808.f) return false;
+  out = __float2ll_rn(s);
+  return true;
+}
+
+// checked_radio_atomic_add's overflow test on the returned previous value
+// (RadioProjection.inl:246-251).
+__device__ __forceinline__ bool checked(unsigned long long previous_bits, long long inc) {
+  long long const previous = static_cast<long long>(previous_bits);
+  return !((inc > 0 && previous > LLONG_MAX - inc) || (inc < 0 && previous < LLONG_MIN - inc));
+}
+
+__device__ __forceinline__ double amp_div(double a, double b) { return a / b; }
+__device__ __forceinline__ float amp_div(float a, float b) { return __fdividef(a, b); }
+
+template <class T>
+__device__ __forceinline__ Vec3<T> scaled(Vec3<T> v, T s) {
+  return {v.x * s, v.y * s, v.z * s};
+}
+
+// ---------------------------------------------------------------- sinks
+// Trace rows of one observer: global X|Y|Z rows already offset to the
+// observer's first bin.
+struct GlobalSink {
+  unsigned long long* row[3];
+  double* frow[3];
+  __device__ __forceinline__ bool add(int c, uint64_t bin, long long v) {
+    return checked(atomicAdd(row[c] + bin, static_cast<unsigned long long>(v)), v);
+  }
+  __device__ __forceinline__ void addf(int c, uint64_t bin, double v) { atomicAdd(frow[c] + bin, v); }
+};
+
+// Shared-memory window of `width` bins starting at bin 0 (rows X|Y|Z), with
+// bins past the window spilled to the global rows.
+struct WindowSink {
+  unsigned long long* win;
+  double* fwin;
+  uint32_t width;
+  unsigned long long* row[3];
+  double* frow[3];
+  __device__ __forceinline__ bool add(int c, uint64_t bin, long long v) {
+    unsigned long long const u = static_cast<unsigned long long>(v);
+    unsigned long long const previous =
+        bin < width ? atomicAdd(win + c * width + bin, u) : atomicAdd(row[c] + bin, u);
+    return checked(previous, v);
+  }
+  __device__ __forceinline__ void addf(int c, uint64_t bin, double v) {
+    if (bin < width)
+      atomicAdd(fwin + c * width + bin, v);
+    else
+      atomicAdd(frow[c] + bin, v);
+  }
+};
+
+// ---------------------------------------------------------------- add_sample
+// RadioProjection.inl:263-301.  kPotential selects the ZHS overload (no time
+// gate).
+template <bool kPotential>
+__device__ __forceinline__ bool sample_bin(ObserverCache const& o, double t, uint64_t& bin) {
+  if (!kPotential) {
+    if (t < o.start_time || t > o.end_time) return false;
+  }
+  double const bv = nearest_bin((t - o.start_time) * o.sample_rate);
+  if (!(bv >= 0. && bv < o.bins_d)) return false;
+  bin = static_cast<uint64_t>(bv);
+  return bin < o.bins;
+}
+
+template <class Amp>
+struct Deposit {
+  Vec3<Amp> value;
+  long long ix, iy, iz;
+  bool okx, oky, okz;
+};
+
+template <bool kFixed, class Amp>
+__device__ __forceinline__ Deposit<Amp> make_deposit(ObserverCache const& o, Vec3<Amp> v) {
+  Deposit<Amp> d;
+  d.value = v;
+  if (kFixed) {
+    d.okx = to_fixed(v.x, o, d.ix);
+    d.oky = to_fixed(v.y, o, d.iy);
+    d.okz = to_fixed(v.z, o, d.iz);
+  }
+  return d;
+}
+
+template <bool kPotential, bool kFixed, class Amp, class Sink>
+__device__ __forceinline__ void deposit(ObserverCache const& o, Sink& sink, double t,
+                                        Deposit<Amp> const& d, unsigned long long& contributions,
+                                        unsigned long long& overflows) {
+  uint64_t bin;
+  if (!sample_bin<kPotential>(o, t, bin)) return;
+  if (kFixed) {
+    bool const ax = d.okx && sink.add(0, bin, d.ix);
+    bool const ay = d.oky && sink.add(1, bin, d.iy);
+    bool const az = d.okz && sink.add(2, bin, d.iz);
+    if (!(ax && ay && az)) {
+      ++overflows;
+      return;
+    }
+  } else {
+    sink.addf(0, bin, static_cast<double>(d.value.x));
+    sink.addf(1, bin, static_cast<double>(d.value.y));
+    sink.addf(2, bin, static_cast<double>(d.value.z));
+  }
+  ++contributions;
+}
+
+template <bool kPotential, bool kFixed, class Amp, class Sink>
+__device__ __forceinline__ void add_sample(ObserverCache const& o, Sink& sink, double t,
+                                           Vec3<Amp> v, unsigned long long& contributions,
+                                           unsigned long long& overflows) {
+  uint64_t bin;
+  if (!sample_bin<kPotential>(o, t, bin)) return;
+  if (kFixed) {
+    long long ix, iy, iz;
+    bool const ax = to_fixed(v.x, o, ix) && sink.add(0, bin, ix);
+    bool const ay = to_fixed(v.y, o, iy) && sink.add(1, bin, iy);
+    bool const az = to_fixed(v.z, o, iz) && sink.add(2, bin, iz);
+    if (!(ax && ay && az)) {
+      ++overflows;
+      return;
+    }
+  } else {
+    sink.addf(0, bin, static_cast<double>(v.x));
+    sink.addf(1, bin, static_cast<double>(v.y));
+    sink.addf(2, bin, static_cast<double>(v.z));
+  }
+  ++contributions;
+}
+
+// ---------------------------------------------------------------- CoREAS
+// accumulate_co_reas, RadioProjection.inl:339-409.
+template <bool kFixed, class Amp, class Sink>
+__device__ __forceinline__ void coreas_pair(Track const& t, Propagation const& p,
+                                            ObserverCache const& o, Sink& sink, Counts& c) {
+  Path const ps = propagate<true>(p, o, t.sx, t.sy, t.sz);
+  Path const pe = propagate<true>(p, o, t.ex, t.ey, t.ez);
+  double const pre = doppler(ps.n_src, t.bx, t.by, t.bz, ps.kx, ps.ky, ps.kz);
+  double const post = doppler(pe.n_src, t.bx, t.by, t.bz, pe.kx, pe.ky, pe.kz);
+  double sr = t.ts + ps.time;
+  double er = t.te + pe.time;
+  double const cf = t.constant * o.sample_rate;
+  Vec3<Amp> const beta{static_cast<Amp>(t.bx), static_cast<Amp>(t.by), static_cast<Amp>(t.bz)};
+
+  if (ps.n_dst > 1. && (fabs(pre) < kCoreasThreshold || fabs(post) < kCoreasThreshold)) {
+    double const mx = (t.sx + t.ex) * 0.5, my = (t.sy + t.ey) * 0.5, mz = (t.sz + t.ez) * 0.5;
+    double const mt = (t.ts + t.te) * 0.5;
+    Path const pm = propagate<true>(p, o, mx, my, mz);
+    double const mr = mt + pm.time;
+    double const md = doppler(pm.n_src, t.bx, t.by, t.bz, pm.kx, pm.ky, pm.kz);
+    Vec3<Amp> const k{static_cast<Amp>(pm.kx), static_cast<Amp>(pm.ky), static_cast<Amp>(pm.kz)};
+    Vec3<Amp> fstart =
+        scaled(cross(k, cross(k, beta)), amp_div(static_cast<Amp>(cf), static_cast<Amp>(md * pm.dist)));
+    Vec3<Amp> fend = scaled(fstart, static_cast<Amp>(-1.));
+    double dt = t.length / (kSpeedOfLight * t.beta_module) * fabs(md);
+    if (sr < er) {
+      sr = mr - 0.5 * dt;
+      er = mr + 0.5 * dt;
+    } else {
+      sr = mr + 0.5 * dt;
+      er = mr - 0.5 * dt;
+    }
+    double const res = o.resolution;
+    dt = er - sr;
+    if (fabs(dt) < res) {
+      Amp const s = static_cast<Amp>(fabs(dt / res));
+      fstart = scaled(fstart, s);
+      fend = scaled(fend, s);
+      separate_same_bin(sr, er, res, true);
+    }
+    add_sample<false, kFixed>(o, sink, sr, fstart, c.coreas, c.overflows);
+    add_sample<false, kFixed>(o, sink, er, fend, c.coreas, c.overflows);
+    return;
+  }
+
+  Vec3<Amp> const ks{static_cast<Amp>(ps.kx), static_cast<Amp>(ps.ky), static_cast<Amp>(ps.kz)};
+  Vec3<Amp> const ke{static_cast<Amp>(pe.kx), static_cast<Amp>(pe.ky), static_cast<Amp>(pe.kz)};
+  Vec3<Amp> fstart =
+      scaled(cross(ks, cross(ks, beta)), amp_div(static_cast<Amp>(cf), static_cast<Amp>(pre * ps.dist)));
+  Vec3<Amp> fend =
+      scaled(cross(ke, cross(ke, beta)), amp_div(static_cast<Amp>(-cf), static_cast<Amp>(post * pe.dist)));
+  if (pre < 1.e-9 || post < 1.e-9) {
+    double const res = o.resolution;
+    double const dt = er - sr;
+    if (fabs(dt) < res) {
+      Amp const s = static_cast<Amp>(fabs(dt / res));
+      fstart = scaled(fstart, s);
+      fend = scaled(fend, s);
+      separate_same_bin(sr, er, res, false);
+    }
+  }
+  add_sample<false, kFixed>(o, sink, sr, fstart, c.coreas, c.overflows);
+  add_sample<false, kFixed>(o, sink, er, fend, c.coreas, c.overflows);
+}
+
+// ---------------------------------------------------------------- ZHS
+// accumulate_zhs_segment, RadioProjection.inl:412-480.
+template <bool kFixed, class Amp, class Sink>
+__device__ __forceinline__ void zhs_segment(double p1x, double p1y, double p1z, double p2x,
+                                            double p2y, double p2z, double t1, double t2,
+                                            Track const& t, Propagation const& p,
+                                            ObserverCache const& o, Sink& sink, Counts& c,
+                                            bool subdivided) {
+  double const mx = (p1x + p2x) * 0.5, my = (p1y + p2y) * 0.5, mz = (p1z + p2z) * 0.5;
+  Path const path = propagate<true>(p, o, mx, my, mz);
+  double const bk = t.bx * path.kx + t.by * path.ky + t.bz * path.kz;
+  double const nbk = path.n_src * bk;
+  double const mt = (t1 + t2) * 0.5;
+  double d1 = t1 + path.time - nbk * (t1 - mt);
+  double d2 = t2 + path.time - nbk * (t2 - mt);
+  double sign = 1.;
+  if (d1 > d2) {
+    double const swap = d1;
+    d1 = d2;
+    d2 = swap;
+    sign = -1.;
+  }
+  double const fs = o.sample_rate;
+  double const x1 = (d1 - o.start_time) * fs;
+  double const x2 = (d2 - o.start_time) * fs;
+  double const sb = floor(x1 + 0.5);
+  double const eb = floor(x2 + 0.5);
+  Vec3<Amp> const k{static_cast<Amp>(path.kx), static_cast<Amp>(path.ky), static_cast<Amp>(path.kz)};
+  Vec3<Amp> const beta{static_cast<Amp>(t.bx), static_cast<Amp>(t.by), static_cast<Amp>(t.bz)};
+  Vec3<Amp> const perp = cross(k, cross(beta, k));
+  double const den = 1. - nbk;
+  double const sc = sign * t.constant;
+  double const dd = den * path.dist;
+
+  if (sb == eb) {
+    Vec3<Amp> pot;
+    if (fabs(den) > 1.e-15) {
+      double const frac = fabs(d2 * fs - d1 * fs);
+      pot = scaled(perp, amp_div(static_cast<Amp>(sc * frac), static_cast<Amp>(dd)));
+    } else {
+      double const frac = (t2 - t1) * fs;
+      pot = scaled(perp, amp_div(static_cast<Amp>(sc * frac), static_cast<Amp>(path.dist)));
+    }
+    add_sample<true, kFixed>(o, sink, d2, pot, c.zhs, c.overflows);
+    return;
+  }
+  int const nb = x86_int(eb - sb);
+  double frac = fabs(sb + 0.5 - x1);
+  add_sample<true, kFixed>(o, sink, d1,
+                           scaled(perp, amp_div(static_cast<Amp>(sc * frac), static_cast<Amp>(dd))),
+                           c.zhs, c.overflows);
+  if (nb > 1) {
+    double const mc = (subdivided ? 1. : sign) * t.constant;
+    Deposit<Amp> const mid =
+        make_deposit<kFixed>(o, scaled(perp, amp_div(static_cast<Amp>(mc), static_cast<Amp>(dd))));
+    // Samples of index i land in bin nearest((d1 + i/fs - t0) fs), monotone in i
+    // and within a hundredth of a bin of x1 + i while all magnitudes stay below
+    // 2^40 bins; indices whose bin is surely outside [0, bins) are skipped,
+    // which changes no sum and no counter.
+    int lo = 1, hi = nb;
+    double const span = 1099511627776.0;  // 2^40
+    if (fabs(x1) < span && fabs(o.start_time * fs) < span && fabs(d1 * fs) < span &&
+        static_cast<double>(nb) < span) {
+      double const first = -x1 - 3.;
+      double const last = o.bins_d - x1 + 3.;
+      if (first > 1.) lo = first >= static_cast<double>(nb) ? nb : static_cast<int>(first);
+      if (last < static_cast<double>(nb)) hi = last <= 1. ? 1 : static_cast<int>(last) + 1;
+      if (hi > nb) hi = nb;
+    }
+    for (int index = lo; index < hi; ++index)
+      deposit<true, kFixed>(o, sink, d1 + static_cast<double>(index) / fs, mid, c.zhs, c.overflows);
+  }
+  frac = fabs(x2 + 0.5 - eb);
+  add_sample<true, kFixed>(o, sink, d2,
+                           scaled(perp, amp_div(static_cast<Amp>(sc * frac), static_cast<Amp>(dd))),
+                           c.zhs, c.overflows);
+}
+
+// accumulate_zhs, RadioProjection.inl:483-529.
+template <bool kFixed, class Amp, class Sink>
+__device__ __forceinline__ void zhs_pair(Track const& t, Propagation const& p,
+                                         ObserverCache const& o, Sink& sink, Counts& c) {
+  double const mx = (t.sx + t.ex) * 0.5, my = (t.sy + t.ey) * 0.5, mz = (t.sz + t.ez) * 0.5;
+  Path const pm = propagate<false>(p, o, mx, my, mz);
+  double const uk = (t.bx * pm.kx + t.by * pm.ky + t.bz * pm.kz) / t.beta_module;
+  double const s2 = 1. - uk * uk;
+  double const fraunhofer = s2 * t.length * t.length / pm.dist / o.wavelength * 2. * kPi;
+  double divisor = 1.;
+  int subtracks = 1;
+  if (fraunhofer > 1.) {
+    divisor = sqrt(fraunhofer) + 1.;
+    subtracks = x86_int(ceil(divisor));
+  }
+  c.subtracks += static_cast<unsigned long long>(static_cast<long long>(subtracks));
+  int const refinement = static_cast<int>(p.refinement);
+  if (subtracks == 1 && refinement == 1) {
+    // divisor is exactly 1: point2 = start + (end - start), time2 likewise
+    zhs_segment<kFixed, Amp>(t.sx, t.sy, t.sz, t.sx + (t.ex - t.sx), t.sy + (t.ey - t.sy),
+                             t.sz + (t.ez - t.sz), t.ts, t.ts + (t.te - t.ts), t, p, o, sink, c,
+                             false);
+    return;
+  }
+  double const rd = static_cast<double>(refinement);
+  double const rx = (t.ex - t.sx) / divisor / rd;
+  double const ry = (t.ey - t.sy) / divisor / rd;
+  double const rz = (t.ez - t.sz) / divisor / rd;
+  double const rt = (t.te - t.ts) / divisor / rd;
+  double p1x = t.sx, p1y = t.sy, p1z = t.sz, t1 = t.ts;
+  for (int index = 0; index < subtracks; ++index) {
+    for (int r = 0; r < refinement; ++r) {
+      double const p2x = p1x + rx, p2y = p1y + ry, p2z = p1z + rz, t2 = t1 + rt;
+      zhs_segment<kFixed, Amp>(p1x, p1y, p1z, p2x, p2y, p2z, t1, t2, t, p, o, sink, c, true);
+      p1x = p2x;
+      p1y = p2y;
+      p1z = p2z;
+      t1 = t2;
+    }
+  }
+  if (refinement > 1)
+    c.subtracks += static_cast<unsigned long long>(
+        static_cast<long long>(subtracks * (refinement - 1)));
+}
+
+// ---------------------------------------------------------------- helpers
+__device__ __forceinline__ Track load_track(const double* __restrict__ base, uint64_t stride,
+                                            uint64_t i) {
+  Track t;
+  t.sx = __ldg(base + kSx * stride + i);
+  t.sy = __ldg(base + kSy * stride + i);
+  t.sz = __ldg(base + kSz * stride + i);
+  t.ex = __ldg(base + kEx * stride + i);
+  t.ey = __ldg(base + kEy * stride + i);
+  t.ez = __ldg(base + kEz * stride + i);
+  t.ts = __ldg(base + kTs * stride + i);
+  t.te = __ldg(base + kTe * stride + i);
+  t.bx = __ldg(base + kBx * stride + i);
+  t.by = __ldg(base + kBy * stride + i);
+  t.bz = __ldg(base + kBz * stride + i);
+  t.length = __ldg(base + kLen * stride + i);
+  t.beta_module = __ldg(base + kBmod * stride + i);
+  t.constant = __ldg(base + kConst * stride + i);
+  return t;
+}
+
+__device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
+  for (int d = 16; d > 0; d >>= 1) v += __shfl_down_sync(0xffffffffu, v, d);
+  return v;
+}
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int d = 16; d > 0; d >>= 1) v += __shfl_down_sync(0xffffffffu, v, d);
+  return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+  for (int d = 16; d > 0; d >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, d));
+  return v;
+}
+
+// Adds per-thread counts into the event counters: one atomic per warp.
+// Every lane of the warp must call it.
+__device__ __forceinline__ void flush_counts(Counts& c, DeviceCounters* counters) {
+  unsigned long long const a = warp_sum(c.coreas), b = warp_sum(c.zhs),
+                           s = warp_sum(c.subtracks), f = warp_sum(c.overflows);
+  if ((threadIdx.x & 31) == 0) {
+    if (a) atomicAdd(&counters->coreas_contributions, a);
+    if (b) atomicAdd(&counters->zhs_contributions, b);
+    if (s) atomicAdd(&counters->zhs_subtracks, s);
+    if (f) atomicAdd(&counters->fixed_point_overflows, f);
+  }
+  c = Counts{};
+}
+
+// RadioAtomicOperations::maximum (RadioAtomicOperations.inl:46-56): finite,
+// non-negative maxima compare as their bit patterns.
+__device__ __forceinline__ void atomic_max_nonnegative(double* address, double value) {
+  atomicMax(reinterpret_cast<unsigned long long*>(address),
+            static_cast<unsigned long long>(__double_as_longlong(value)));
+}
+
+// diagnostic_energy_bin, RadioProjection.inl:531-538.
+__device__ __forceinline__ int energy_bin(double kinetic) {
+  double const edges[14] = {1.e-3, 2.e-3, 5.e-3, 1.e-2, 2.e-2, 5.e-2, 1.e-1,
+                            2.e-1, 5.e-1, 1.,    2.,    5.,    10.,   100.};
+  int index = 0;
+  while (index < 14 && kinetic > edges[index]) ++index;
+  return index;
+}
+
+// ---------------------------------------------------------------- ingest
+__global__ void __launch_bounds__(256) ingest_kernel(
+    const c8r_lepton_transport_record* __restrict__ records, uint64_t count,
+    double* __restrict__ tracks, uint64_t stride, unsigned long long* slot,
+    DeviceCounters* counters, int diagnostics) {
+  uint64_t const i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  bool valid = false;
+  Track t;
+  double duration = 0.;
+  c8r_particle_state const* s = nullptr;
+  c8r_particle_state const* e = nullptr;
+  if (i < count) {
+    s = &records[i].start;
+    e = &records[i].end;
+    int const pid = s->pid;
+    // make_radio_track_kinematics, RadioProjection.inl:145-168
+    if (pid == 11 || pid == -11) {
+      t.sx = s->position_m[0];
+      t.sy = s->position_m[1];
+      t.sz = s->position_m[2];
+      t.ex = e->position_m[0];
+      t.ey = e->position_m[1];
+      t.ez = e->position_m[2];
+      t.ts = s->time_s;
+      t.te = e->time_s;
+      duration = t.te - t.ts;
+      double const dx = t.ex - t.sx, dy = t.ey - t.sy, dz = t.ez - t.sz;
+      t.length = sqrt(dx * dx + dy * dy + dz * dz);
+      if (duration > 0. && t.length > 0.) {
+        double const denominator = kSpeedOfLight * duration;
+        t.bx = dx / denominator;
+        t.by = dy / denominator;
+        t.bz = dz / denominator;
+        t.beta_module = t.length / (kSpeedOfLight * duration);
+        double const charge = pid == 11 ? -kElementaryCharge : kElementaryCharge;
+        t.constant = charge * kEmConstant * s->weight;
+        valid = true;
+      }
+    }
+  }
+  unsigned const ballot = __ballot_sync(0xffffffffu, valid);
+  unsigned const lane = threadIdx.x & 31;
+  unsigned long long base = 0;
+  if (lane == 0 && ballot) base = atomicAdd(slot, static_cast<unsigned long long>(__popc(ballot)));
+  base = __shfl_sync(0xffffffffu, base, 0);
+  if (valid) {
+    uint64_t const j = base + __popc(ballot & ((1u << lane) - 1u));
+    tracks[kSx * stride + j] = t.sx;
+    tracks[kSy * stride + j] = t.sy;
+    tracks[kSz * stride + j] = t.sz;
+    tracks[kEx * stride + j] = t.ex;
+    tracks[kEy * stride + j] = t.ey;
+    tracks[kEz * stride + j] = t.ez;
+    tracks[kTs * stride + j] = t.ts;
+    tracks[kTe * stride + j] = t.te;
+    tracks[kBx * stride + j] = t.bx;
+    tracks[kBy * stride + j] = t.by;
+    tracks[kBz * stride + j] = t.bz;
+    tracks[kLen * stride + j] = t.length;
+    tracks[kBmod * stride + j] = t.beta_module;
+    tracks[kConst * stride + j] = t.constant;
+  }
+  if (lane == 0 && ballot) atomicAdd(&counters->valid_tracks, static_cast<unsigned long long>(__popc(ballot)));
+  if (!diagnostics) return;
+
+  // record_track diagnostics, RadioProjection.inl:553-610 (warp-reduced).
+  double w = 0., len = 0., wl = 0., ewl = 0., el = 0., pl = 0., sl = 0., dchg = 0., dchg2 = 0.,
+         bdef = 0., tres = 0., maxlen = 0., maxchg = 0., sdx = 0., sdy = 0., sdz = 0.;
+  int ebin = -1;
+  double ebin_value = 0.;
+  if (valid) {
+    double const weight = s->weight;
+    double const kinetic = s->energy_gev - kElectronMassGeV;
+    if (isfinite(t.length) && t.length > 0. && isfinite(weight) && !(weight < 0.) &&
+        isfinite(kinetic) && !(kinetic < 0.)) {
+      double const weighted_length = weight * t.length;
+      w = weight;
+      len = t.length;
+      wl = weighted_length;
+      ewl = weighted_length * kinetic;
+      maxlen = t.length;
+      if (s->pid == 11) {
+        el = weighted_length;
+        sl = -weighted_length;
+      } else {
+        pl = weighted_length;
+        sl = weighted_length;
+      }
+      ebin = energy_bin(kinetic);
+      ebin_value = weighted_length;
+      double direction_dot = 0.;
+      double delta[3];
+      for (int axis = 0; axis < 3; ++axis) {
+        double const pre = s->direction[axis];
+        double const post = e->direction[axis];
+        direction_dot += pre * post;
+        delta[axis] = post - pre;
+      }
+      double clamped = -1. > direction_dot ? -1. : direction_dot;
+      clamped = 1. < clamped ? 1. : clamped;
+      double const change = acos(clamped);
+      double const residual = duration - t.length / kSpeedOfLight;
+      dchg = weight * change;
+      dchg2 = weight * change * change;
+      bdef = weighted_length * (1. - t.beta_module);
+      tres = weight * residual;
+      maxchg = change;
+      double const charge_sign = s->pid == 11 ? -1. : 1.;
+      sdx = charge_sign * weight * delta[0];
+      sdy = charge_sign * weight * delta[1];
+      sdz = charge_sign * weight * delta[2];
+    }
+  }
+  w = warp_sum(w);
+  len = warp_sum(len);
+  wl = warp_sum(wl);
+  ewl = warp_sum(ewl);
+  el = warp_sum(el);
+  pl = warp_sum(pl);
+  sl = warp_sum(sl);
+  dchg = warp_sum(dchg);
+  dchg2 = warp_sum(dchg2);
+  bdef = warp_sum(bdef);
+  tres = warp_sum(tres);
+  sdx = warp_sum(sdx);
+  sdy = warp_sum(sdy);
+  sdz = warp_sum(sdz);
+  maxlen = warp_max(maxlen);
+  maxchg = warp_max(maxchg);
+  if (lane == 0 && ballot) {
+    atomicAdd(&counters->weighted_segment_count, w);
+    atomicAdd(&counters->track_length_m, len);
+    atomicAdd(&counters->weighted_track_length_m, wl);
+    atomicAdd(&counters->energy_weighted_track_length_gev_m, ewl);
+    atomicAdd(&counters->electron_weighted_track_length_m, el);
+    atomicAdd(&counters->positron_weighted_track_length_m, pl);
+    atomicAdd(&counters->signed_charge_weighted_track_length_m, sl);
+    atomicAdd(&counters->weighted_direction_change_rad, dchg);
+    atomicAdd(&counters->weighted_direction_change_squared_rad2, dchg2);
+    atomicAdd(&counters->weighted_beta_deficit_track_length_m, bdef);
+    atomicAdd(&counters->weighted_time_residual_s, tres);
+    atomicAdd(&counters->signed_charge_weighted_direction_change[0], sdx);
+    atomicAdd(&counters->signed_charge_weighted_direction_change[1], sdy);
+    atomicAdd(&counters->signed_charge_weighted_direction_change[2], sdz);
+    atomic_max_nonnegative(&counters->maximum_segment_length_m, maxlen);
+    atomic_max_nonnegative(&counters->maximum_direction_change_rad, maxchg);
+  }
+  if (ebin >= 0) atomicAdd(&counters->weighted_track_length_by_kinetic_energy_m[ebin], ebin_value);
+}
+
+// ---------------------------------------------------------------- direct
+template <bool kFixed, class Amp, bool kCoreas, bool kZhs>
+__global__ void __launch_bounds__(256) direct_kernel(EventPlan ev) {
+  uint64_t const tracks = *ev.valid_tracks;
+  uint32_t const observers =
+      ev.observer_count[0] > ev.observer_count[1] ? ev.observer_count[0] : ev.observer_count[1];
+  uint64_t const pairs = tracks * observers;
+  Counts c;
+  for (uint64_t pair = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; pair < pairs;
+       pair += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    uint64_t const ti = pair / observers;
+    uint32_t const oi = static_cast<uint32_t>(pair - ti * observers);
+    Track const t = load_track(ev.tracks, ev.stride, ti);
+    if (kCoreas && oi < ev.observer_count[0]) {
+      ObserverCache const& o = ev.observers[0][oi];
+      GlobalSink sink;
+      for (int r = 0; r < 3; ++r) {
+        sink.row[r] = kFixed ? ev.fixed[0] + r * ev.total_bins[0] + o.offset : nullptr;
+        sink.frow[r] = kFixed ? nullptr : ev.floating[0] + r * ev.total_bins[0] + o.offset;
+      }
+      coreas_pair<kFixed, Amp>(t, ev.propagation, o, sink, c);
+    }
+    if (kZhs && oi < ev.observer_count[1]) {
+      ObserverCache const& o = ev.observers[1][oi];
+      GlobalSink sink;
+      for (int r = 0; r < 3; ++r) {
+        sink.row[r] = kFixed ? ev.fixed[1] + r * ev.total_bins[1] + o.offset : nullptr;
+        sink.frow[r] = kFixed ? nullptr : ev.floating[1] + r * ev.total_bins[1] + o.offset;
+      }
+      zhs_pair<kFixed, Amp>(t, ev.propagation, o, sink, c);
+    }
+  }
+  flush_counts(c, ev.counters);
+}
+
+// ---------------------------------------------------------------- windowed
+constexpr int kWindowThreadsMax = 512;
+
+__device__ __forceinline__ uint32_t find_event(EventPlan const* events, uint32_t n, uint64_t item) {
+  uint32_t lo = 0, hi = n;  // last event with first_item <= item
+  while (hi - lo > 1) {
+    uint32_t const mid = (lo + hi) >> 1;
+    if (events[mid].first_item <= item)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+template <bool kFixed, class Amp>
+__global__ void __launch_bounds__(kWindowThreadsMax, 1)
+    windowed_kernel(const __grid_constant__ WorkPlan plan) {
+  extern __shared__ __align__(16) unsigned long long window[];
+  __shared__ unsigned long long item_shared;
+  Counts c;
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) item_shared = atomicAdd(plan.next_item, 1u);
+    __syncthreads();
+    uint64_t const item = item_shared;
+    if (item >= plan.total_items) break;
+    EventPlan const& ev = plan.events[find_event(plan.events, plan.event_count, item)];
+    uint64_t const local = item - ev.first_item;
+    uint32_t const per_chunk = ev.observer_count[0] + ev.observer_count[1];
+    uint64_t const chunk = local / per_chunk;
+    uint32_t const r = static_cast<uint32_t>(local - chunk * per_chunk);
+    int const algorithm = r < ev.observer_count[0] ? 0 : 1;
+    uint32_t const oi = algorithm ? r - ev.observer_count[0] : r;
+    uint64_t const track_count = *ev.valid_tracks;
+    uint64_t const begin = chunk * ev.chunk_size;
+    if (begin >= track_count) continue;
+    uint64_t const end = begin + ev.chunk_size < track_count ? begin + ev.chunk_size : track_count;
+    ObserverCache const o = ev.observers[algorithm][oi];
+    uint32_t const width = static_cast<uint32_t>(o.bins < ev.window ? o.bins : ev.window);
+
+    // zero the window (3 rows of width bins)
+    for (uint32_t j = threadIdx.x; j < 3 * width; j += blockDim.x) window[j] = 0ull;
+    __syncthreads();
+
+    WindowSink sink;
+    sink.win = window;
+    sink.fwin = reinterpret_cast<double*>(window);
+    sink.width = width;
+    uint64_t const total = ev.total_bins[algorithm];
+    for (int row = 0; row < 3; ++row) {
+      sink.row[row] = kFixed ? ev.fixed[algorithm] + row * total + o.offset : nullptr;
+      sink.frow[row] = kFixed ? nullptr : ev.floating[algorithm] + row * total + o.offset;
+    }
+    if (algorithm == 0) {
+      for (uint64_t i = begin + threadIdx.x; i < end; i += blockDim.x)
+        coreas_pair<kFixed, Amp>(load_track(ev.tracks, ev.stride, i), ev.propagation, o, sink, c);
+    } else {
+      for (uint64_t i = begin + threadIdx.x; i < end; i += blockDim.x)
+        zhs_pair<kFixed, Amp>(load_track(ev.tracks, ev.stride, i), ev.propagation, o, sink, c);
+    }
+    __syncthreads();
+
+    // flush: non-zero bins, checked global adds
+    for (uint32_t j = threadIdx.x; j < 3 * width; j += blockDim.x) {
+      unsigned long long const v = window[j];
+      if (v == 0ull) continue;
+      uint32_t const row = j / width;
+      uint32_t const bin = j - row * width;
+      if (kFixed) {
+        long long const inc = static_cast<long long>(v);
+        if (!checked(atomicAdd(sink.row[row] + bin, v), inc)) ++c.overflows;
+      } else {
+        atomicAdd(sink.frow[row] + bin, __longlong_as_double(static_cast<long long>(v)));
+      }
+    }
+    flush_counts(c, ev.counters);
+  }
+}
+
+// ---------------------------------------------------------------- decode
+__global__ void decode_kernel(const long long* __restrict__ fixed, double* __restrict__ out,
+                              uint64_t total_bins, const uint64_t* __restrict__ offsets,
+                              const double* __restrict__ factors) {
+  uint32_t const o = blockIdx.y;
+  uint64_t const begin = offsets[o], end = offsets[o + 1];
+  double const f = factors[o];
+  for (uint64_t i = begin + static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < end;
+       i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    out[i] = static_cast<double>(fixed[i]) * f;
+    out[total_bins + i] = static_cast<double>(fixed[total_bins + i]) * f;
+    out[2 * total_bins + i] = static_cast<double>(fixed[2 * total_bins + i]) * f;
+  }
+}
+
+template <bool kFixed, class Amp>
+cudaError_t direct_dispatch(EventPlan const& ev, uint64_t bound, bool coreas, bool zhs,
+                            cudaStream_t stream) {
+  uint32_t const observers =
+      ev.observer_count[0] > ev.observer_count[1] ? ev.observer_count[0] : ev.observer_count[1];
+  uint64_t const pairs = bound * observers;
+  if (pairs == 0) return cudaSuccess;
+  int device = 0, sms = 148;
+  cudaGetDevice(&device);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  uint64_t blocks = (pairs + 255) / 256;
+  uint64_t const cap = static_cast<uint64_t>(sms) * 16;
+  if (blocks > cap) blocks = cap;
+  unsigned const grid = static_cast<unsigned>(blocks);
+  if (coreas && zhs)
+    direct_kernel<kFixed, Amp, true, true><<<grid, 256, 0, stream>>>(ev);
+  else if (coreas)
+    direct_kernel<kFixed, Amp, true, false><<<grid, 256, 0, stream>>>(ev);
+  else if (zhs)
+    direct_kernel<kFixed, Amp, false, true><<<grid, 256, 0, stream>>>(ev);
+  return cudaGetLastError();
+}
+
+template <bool kFixed, class Amp>
+cudaError_t windowed_dispatch(WorkPlan const& plan, int ctas, int threads, cudaStream_t stream) {
+  size_t const bytes = static_cast<size_t>(plan.window) * 3 * sizeof(unsigned long long);
+  cudaError_t err = cudaFuncSetAttribute(windowed_kernel<kFixed, Amp>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(bytes));
+  if (err != cudaSuccess) return err;
+  windowed_kernel<kFixed, Amp><<<ctas, threads, bytes, stream>>>(plan);
+  return cudaGetLastError();
+}
+
+template <bool kFixed, class Amp>
+int ctas_per_sm(int window, int threads) {
+  size_t const bytes = static_cast<size_t>(window) * 3 * sizeof(unsigned long long);
+  cudaFuncSetAttribute(windowed_kernel<kFixed, Amp>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       static_cast<int>(bytes));
+  int blocks = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, windowed_kernel<kFixed, Amp>, threads,
+                                                    bytes) != cudaSuccess)
+    return 0;
+  return blocks;
+}
+
+}  // namespace
+
+cudaError_t launch_ingest(const c8r_lepton_transport_record* records, uint64_t count,
+                          double* tracks, uint64_t stride, unsigned long long* slot,
+                          DeviceCounters* counters, bool diagnostics, cudaStream_t stream) {
+  if (count == 0) return cudaSuccess;
+  uint64_t const blocks = (count + 255) / 256;
+  ingest_kernel<<<static_cast<unsigned>(blocks), 256, 0, stream>>>(records, count, tracks, stride,
+                                                                   slot, counters, diagnostics);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_direct(EventPlan const& event, uint64_t track_bound, bool coreas, bool zhs,
+                          bool fixed, Precision precision, cudaStream_t stream) {
+  if (fixed) {
+    return precision == Precision::kFP64
+               ? direct_dispatch<true, double>(event, track_bound, coreas, zhs, stream)
+               : direct_dispatch<true, float>(event, track_bound, coreas, zhs, stream);
+  }
+  return precision == Precision::kFP64
+             ? direct_dispatch<false, double>(event, track_bound, coreas, zhs, stream)
+             : direct_dispatch<false, float>(event, track_bound, coreas, zhs, stream);
+}
+
+cudaError_t launch_windowed(WorkPlan const& plan, bool fixed, Precision precision, int ctas,
+                            int threads, cudaStream_t stream) {
+  if (plan.total_items == 0) return cudaSuccess;
+  if (fixed)
+    return precision == Precision::kFP64 ? windowed_dispatch<true, double>(plan, ctas, threads, stream)
+                                         : windowed_dispatch<true, float>(plan, ctas, threads, stream);
+  return precision == Precision::kFP64 ? windowed_dispatch<false, double>(plan, ctas, threads, stream)
+                                       : windowed_dispatch<false, float>(plan, ctas, threads, stream);
+}
+
+int windowed_max_bins(int device) {
+  int optin = 0;
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+  // static shared memory of the kernel is a handful of bytes; keep 1 KiB spare
+  int const usable = optin - 1024;
+  return usable > 0 ? usable / static_cast<int>(3 * sizeof(unsigned long long)) : 0;
+}
+
+int windowed_ctas_per_sm(int window, int threads, bool fixed, Precision precision) {
+  if (fixed)
+    return precision == Precision::kFP64 ? ctas_per_sm<true, double>(window, threads)
+                                         : ctas_per_sm<true, float>(window, threads);
+  return precision == Precision::kFP64 ? ctas_per_sm<false, double>(window, threads)
+                                       : ctas_per_sm<false, float>(window, threads);
+}
+
+cudaError_t launch_decode(const long long* fixed, double* out, uint64_t total_bins,
+                          const uint64_t* observer_offsets, const double* factors,
+                          uint32_t observer_count, uint64_t max_bins, cudaStream_t stream) {
+  if (observer_count == 0 || total_bins == 0) return cudaSuccess;
+  uint64_t bx = (max_bins + 255) / 256;
+  if (bx > 64) bx = 64;
+  if (bx == 0) bx = 1;
+  dim3 const grid(static_cast<unsigned>(bx), observer_count);
+  decode_kernel<<<grid, 256, 0, stream>>>(fixed, out, total_bins, observer_offsets, factors);
+  return cudaGetLastError();
+}
+
+}  // namespace c8r

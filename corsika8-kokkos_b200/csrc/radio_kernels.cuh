@@ -1,0 +1,102 @@
+// radio_kernels.cuh — launch-side declarations shared by the host library.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "radio_device.cuh"
+
+struct c8r_lepton_transport_record;
+struct c8r_counters;
+
+namespace c8r {
+
+// Device-side counters of one event (the layout of RadioCounters).
+struct alignas(8) DeviceCounters {
+  unsigned long long coreas_contributions;
+  unsigned long long zhs_contributions;
+  unsigned long long zhs_subtracks;
+  unsigned long long valid_tracks;
+  unsigned long long fixed_point_overflows;
+  double weighted_segment_count;
+  double track_length_m;
+  double weighted_track_length_m;
+  double electron_weighted_track_length_m;
+  double positron_weighted_track_length_m;
+  double signed_charge_weighted_track_length_m;
+  double energy_weighted_track_length_gev_m;
+  double maximum_segment_length_m;
+  double weighted_direction_change_rad;
+  double weighted_direction_change_squared_rad2;
+  double weighted_beta_deficit_track_length_m;
+  double weighted_time_residual_s;
+  double maximum_direction_change_rad;
+  double signed_charge_weighted_direction_change[3];
+  double weighted_track_length_by_kinetic_energy_m[15];
+};
+static_assert(sizeof(DeviceCounters) == 288, "RadioCounters layout");
+
+// One event of a projection launch: its tracks (SoA, `stride` doubles per
+// row), observers, traces and counters.  Algorithm 0 = CoREAS field,
+// algorithm 1 = ZHS potential.  Trace rows are [X | Y | Z] of total_bins each.
+struct EventPlan {
+  const double* tracks;
+  uint64_t stride;
+  const unsigned long long* valid_tracks;  // device: tracks written by ingest
+  const ObserverCache* observers[2];
+  uint32_t observer_count[2];
+  unsigned long long* fixed[2];  // int64 fixed-point traces (deterministic)
+  double* floating[2];           // FP64 traces (floating mode)
+  uint64_t total_bins[2];
+  Propagation propagation;
+  DeviceCounters* counters;
+  uint64_t first_item;           // work-list offset of this event
+  uint32_t chunk_size;           // tracks per work item
+  uint32_t chunks;
+  uint32_t window;               // shared-memory bins per item (<= kernel window)
+  uint32_t pad_;
+};
+
+// Persistent windowed launch over a work list of (event, chunk, algorithm,
+// observer) items drawn from an atomic counter.  Passed as a __grid_constant__
+// kernel parameter (no host-to-device copy; graph-capturable).
+constexpr int kMaxEventsPerLaunch = 64;
+constexpr int kWindowThreads = 512;  // upper bound of the windowed block size
+struct WorkPlan {
+  EventPlan events[kMaxEventsPerLaunch];
+  uint32_t event_count;
+  uint32_t window;          // shared-memory bins per CTA (max over events)
+  uint64_t total_items;
+  unsigned int* next_item;  // zeroed before each launch
+};
+
+enum class Precision : int { kFP64 = 0, kMixed = 1 };
+
+// Record ingest: LeptonTransportRecord AoS -> compacted SoA kinematics
+// (make_radio_track_kinematics + record_track).  `slot` receives the number of
+// valid tracks written.
+cudaError_t launch_ingest(const c8r_lepton_transport_record* records, uint64_t count,
+                          double* tracks, uint64_t stride, unsigned long long* slot,
+                          DeviceCounters* counters, bool diagnostics, cudaStream_t stream);
+
+// Direct pair kernel: one thread per (track, observer) pair, global atomics.
+// The valid-track count is read on the device; `track_bound` (the record
+// count) bounds the grid on the host.
+cudaError_t launch_direct(EventPlan const& event, uint64_t track_bound, bool coreas, bool zhs,
+                          bool fixed, Precision precision, cudaStream_t stream);
+
+// Persistent windowed kernel.  `ctas` persistent CTAs of `threads` threads.
+cudaError_t launch_windowed(WorkPlan const& plan, bool fixed, Precision precision, int ctas,
+                            int threads, cudaStream_t stream);
+// Largest window (bins) that fits the opt-in shared memory of this device.
+int windowed_max_bins(int device);
+// Resident CTAs per SM of the windowed kernel for a window and block size.
+int windowed_ctas_per_sm(int window, int threads, bool fixed, Precision precision);
+
+// Fixed-point decode on the device: out[r*bins + i] = in[r*bins + i] * factor(observer).
+cudaError_t launch_decode(const long long* fixed, double* out, uint64_t total_bins,
+                          const uint64_t* observer_offsets, const double* factors,
+                          uint32_t observer_count, uint64_t max_bins, cudaStream_t stream);
+
+}  // namespace c8r

@@ -1,0 +1,260 @@
+/*
+ * c8radio.h — C ABI of the B200 radio projection library (libc8radio.so).
+ *
+ * Drop-in boundary for the CORSIKA8-kokkos radio hot path: CoREAS endpoint
+ * fields and ZHS vector potentials of every electron/positron track segment
+ * at every antenna, binned into antenna time traces.  The entry points below
+ * replace the member functions of corsika::kokkos::radio::RadioAccumulator
+ * (corsika/kokkos/radio/RadioAccumulator.hpp:59-145) behind IRadioBackend
+ * (corsika/kokkos/radio/IRadioBackend.hpp:29-41).  Every function returns a
+ * C8R_* status; the C++ shim c8radio.hpp turns these back into the
+ * reference's exception classes.
+ *
+ * Plain C, plain pointers and sizes.  The record, observer, propagation and
+ * counter structs keep the reference's byte layouts so device producers and
+ * host callers need no conversion.
+ */
+#ifndef C8RADIO_H
+#define C8RADIO_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (one per reference exception class) -------------------- */
+enum {
+  C8R_OK = 0,
+  C8R_INVALID_ARGUMENT = 1, /* std::invalid_argument */
+  C8R_LOGIC_ERROR = 2,      /* std::logic_error */
+  C8R_OUT_OF_RANGE = 3,     /* std::out_of_range */
+  C8R_RUNTIME_ERROR = 4,    /* std::runtime_error (fixed-point overflow) */
+  C8R_LENGTH_ERROR = 5,     /* std::length_error */
+  C8R_OVERFLOW_ERROR = 6,   /* std::overflow_error */
+  C8R_CUDA_ERROR = 7,       /* CUDA runtime failure (message holds the CUDA string) */
+  C8R_BAD_ALLOC = 8         /* device or pinned host allocation failed */
+};
+
+/* ---- record layout: corsika/kokkos/data/ParticleState.hpp:24-44 ----------- */
+typedef struct c8r_particle_state {
+  int32_t pid;           /* signed PDG id: 11 e-, -11 e+ */
+  int32_t medium_id;
+  uint32_t generation;
+  uint32_t reserved;
+  double energy_gev;     /* total energy */
+  double position_m[3];
+  double direction[3];
+  double time_s;
+  double weight;
+  uint64_t history_id;
+  uint64_t parent_history_id;
+  uint64_t step_id;
+  int32_t environment_node;
+  int32_t pad_[3];
+} c8r_particle_state; /* 128 bytes (alignas(16) in the reference) */
+
+/* corsika/kokkos/em/LeptonTransportRecord.hpp:38-70 (752 bytes).  Only start
+ * and end are read by radio projection; the leading InteractionRecord (320 B)
+ * and the trailing transport fields (176 B) are carried opaque. */
+typedef struct c8r_lepton_transport_record {
+  unsigned char interaction[320];
+  c8r_particle_state start;
+  c8r_particle_state end;
+  unsigned char transport[176];
+} c8r_lepton_transport_record;
+
+/* ---- configuration: corsika/kokkos/radio/RadioObserverSnapshot.hpp:17-23 -- */
+typedef struct c8r_observer_snapshot {
+  double position_m[3];
+  double start_time_s;
+  double duration_s;
+  double sample_rate_hz;
+  uint64_t number_of_bins;
+} c8r_observer_snapshot;
+
+/* corsika/kokkos/radio/FlatAtmosphereRadioSnapshot.hpp:20-36; the two tables
+ * are borrowed host arrays of table_size doubles (copied by c8r_create). */
+typedef struct c8r_propagation_snapshot {
+  double homogeneous_refractive_index; /* >0 selects n R / c, no table */
+  double minimum_height_m;
+  double maximum_height_m;
+  double step_m;
+  double inverse_step_per_m;
+  double slope_refractivity_lower;
+  double slope_integrated_refractivity_lower;
+  double slope_refractivity_upper;
+  double slope_integrated_refractivity_upper;
+  const double* refractivity;
+  const double* integrated_refractivity;
+  uint64_t table_size;
+} c8r_propagation_snapshot;
+
+/* Arithmetic of the projection kernels. */
+enum {
+  C8R_PRECISION_FP64 = 0,  /* every expression in FP64, operation for operation as
+                              the reference: the plain drop-in */
+  C8R_PRECISION_MIXED = 1  /* arrival times, distances, emission directions and
+                              1 - n beta.k in FP64 (bin indices and branches are
+                              identical); field and potential amplitudes in FP32 */
+};
+
+/* Kernel family used by accumulate. */
+enum {
+  C8R_KERNEL_AUTO = 0,     /* windowed when the trace window fits, else direct */
+  C8R_KERNEL_DIRECT = 1,   /* one thread per (track, antenna) pair, global 64-bit
+                              atomics per sample: the reference's launch shape */
+  C8R_KERNEL_WINDOWED = 2  /* CTA owns one antenna's trace in shared memory for a
+                              chunk of tracks; flushed with checked global atomics */
+};
+
+/* corsika/kokkos/radio/RadioConfig.hpp:21-53 */
+typedef struct c8r_config {
+  int32_t enabled;
+  int32_t coreas_enabled;
+  int32_t zhs_enabled;
+  int32_t deterministic;      /* 1: int64 fixed-point traces (production default) */
+  double fixed_point_field_limit_v_per_m;
+  int32_t track_diagnostics;
+  uint32_t zhs_subtrack_refinement; /* [1, 64] */
+  c8r_propagation_snapshot propagation;
+  const c8r_observer_snapshot* coreas_observers;
+  uint64_t coreas_observer_count;
+  const c8r_observer_snapshot* zhs_observers;
+  uint64_t zhs_observer_count;
+  /* B200 extensions (zero keeps the defaults). */
+  int32_t precision;          /* C8R_PRECISION_* */
+  int32_t kernel;             /* C8R_KERNEL_* */
+} c8r_config;
+
+/* corsika/kokkos/runtime/TuningParameters.hpp:14-21; zero keeps defaults.
+ * track_tile_size = tracks per windowed CTA chunk, observer_tile_size = bins
+ * per shared-memory window, team_size = threads per CTA. */
+typedef struct c8r_tuning {
+  uint64_t batch_size;
+  uint64_t chunk_size;
+  uint64_t team_size;
+  uint64_t track_tile_size;
+  uint64_t observer_tile_size;
+  uint64_t device_queues;
+} c8r_tuning;
+
+/* corsika/kokkos/radio/RadioProjectionData.hpp:75-96 (288 bytes). */
+typedef struct c8r_counters {
+  unsigned long long coreas_contributions;
+  unsigned long long zhs_contributions;
+  unsigned long long zhs_subtracks;
+  unsigned long long valid_tracks;
+  unsigned long long fixed_point_overflows;
+  double weighted_segment_count;
+  double track_length_m;
+  double weighted_track_length_m;
+  double electron_weighted_track_length_m;
+  double positron_weighted_track_length_m;
+  double signed_charge_weighted_track_length_m;
+  double energy_weighted_track_length_gev_m;
+  double maximum_segment_length_m;
+  double weighted_direction_change_rad;
+  double weighted_direction_change_squared_rad2;
+  double weighted_beta_deficit_track_length_m;
+  double weighted_time_residual_s;
+  double maximum_direction_change_rad;
+  double signed_charge_weighted_direction_change[3];
+  double weighted_track_length_by_kinetic_energy_m[15];
+} c8r_counters;
+
+/* corsika/kokkos/radio/RadioStatistics.hpp:17-63 (the fields this path fills). */
+typedef struct c8r_statistics {
+  uint64_t lepton_tracks;
+  uint64_t track_observer_pairs;
+  uint64_t fused_track_observer_pairs;
+  uint64_t coreas_contributions;
+  uint64_t zhs_contributions;
+  uint64_t zhs_subtracks;
+  uint64_t fixed_point_overflows;
+  uint64_t device_bytes;
+  uint64_t host_to_device_bytes;
+  uint64_t host_tracks_enqueued;
+  uint64_t host_track_batches;
+  uint64_t device_to_host_bytes;
+  uint64_t track_precompute_batches;
+  uint64_t track_precomputed_records;
+  uint64_t direct_projection_batches;
+  uint64_t direct_projection_records;
+  uint64_t projection_tiles;
+  uint64_t track_workspace_bytes;
+  uint64_t maximum_track_batch;
+  uint32_t track_tile_size;
+  uint32_t observer_tile_size;
+  double kernel_time_ms;      /* CUDA-event time of projection kernels (if timing on) */
+  c8r_counters counters;      /* last downloaded device counters */
+} c8r_statistics;
+
+typedef struct c8r_accumulator c8r_accumulator;
+
+/* Library identity and error text. */
+const char* c8r_version(void);
+/* Message of the last failing call on this handle (never NULL). */
+const char* c8r_last_error(const c8r_accumulator* handle);
+/* Message of the last failing call that had no handle (create, validate). */
+const char* c8r_last_global_error(void);
+
+/* RadioAccumulator::validate (RadioAccumulator.inl:931-974). */
+int c8r_config_validate(const c8r_config* config);
+/* RadioAccumulator::projectedDeviceBytes (RadioAccumulator.inl:87-141). */
+int c8r_projected_device_bytes(const c8r_config* config, size_t* bytes);
+
+/* RadioAccumulator::initialize (RadioAccumulator.inl:143-217).  stream is a
+ * cudaStream_t (NULL = legacy default stream); all work is ordered on it. */
+int c8r_create(const c8r_config* config, const c8r_tuning* tuning, void* stream,
+               c8r_accumulator** handle);
+/* Releases device memory after completing queued work.  NULL is ignored. */
+void c8r_destroy(c8r_accumulator* handle);
+
+/* RadioAccumulator::enabled (RadioAccumulator.inl:219-222). */
+int c8r_enabled(const c8r_accumulator* handle, int* enabled);
+/* RadioAccumulator::reset (RadioAccumulator.inl:224-250). */
+int c8r_reset(c8r_accumulator* handle);
+/* RadioAccumulator::enqueueHostLeptonTracks (RadioAccumulator.inl:252-272):
+ * copies before returning; full 4096-record batches are flushed. */
+int c8r_enqueue_host(c8r_accumulator* handle, const c8r_lepton_transport_record* records,
+                     size_t count);
+/* RadioAccumulator::flushHostLeptonTracks (RadioAccumulator.inl:274-290). */
+int c8r_flush(c8r_accumulator* handle);
+/* RadioAccumulator::accumulateLeptonTracks (RadioAccumulator.inl:292-357):
+ * records is DEVICE memory holding extent records, borrowed until the
+ * queued work completes; count > extent is C8R_OUT_OF_RANGE. */
+int c8r_accumulate_device(c8r_accumulator* handle,
+                          const c8r_lepton_transport_record* records, size_t count,
+                          size_t extent);
+/* RadioAccumulator::download (RadioAccumulator.inl:407-439).  Writes decoded
+ * traces in the reference's SoA order [X: all bins | Y | Z] per algorithm
+ * (RadioAccumulator.inl:570-589); each buffer holds 3 * total_bins doubles and
+ * may be NULL when the algorithm has no observers.  counters may be NULL. */
+int c8r_download(c8r_accumulator* handle, double* coreas_xyz, double* zhs_xyz,
+                 c8r_counters* counters);
+/* RadioAccumulator::downloadFixed (RadioAccumulator.inl:359-405): raw int64
+ * fixed-point traces, same layout; requires deterministic mode. */
+int c8r_download_fixed(c8r_accumulator* handle, long long* coreas_xyz, long long* zhs_xyz,
+                       c8r_counters* counters);
+/* Total bins (sum over observers) of each algorithm's traces. */
+int c8r_total_bins(const c8r_accumulator* handle, size_t* coreas_bins, size_t* zhs_bins);
+
+/* RadioAccumulator::statistics / deviceBytes / staticHostToDeviceBytes. */
+int c8r_get_statistics(const c8r_accumulator* handle, c8r_statistics* statistics);
+int c8r_device_bytes(const c8r_accumulator* handle, size_t* bytes);
+int c8r_static_host_to_device_bytes(const c8r_accumulator* handle, size_t* bytes);
+/* RadioAccumulator::reserveTrackCapacity / projectedTrackCapacity
+ * (RadioAccumulator.inl:478-508). */
+int c8r_reserve(c8r_accumulator* handle, size_t count);
+int c8r_projected_track_capacity(const c8r_accumulator* handle, size_t count,
+                                 size_t* retained_bytes, size_t* transient_peak_bytes);
+/* Blocks until all work queued on the accumulator's stream has completed. */
+int c8r_synchronize(c8r_accumulator* handle);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* C8RADIO_H */
