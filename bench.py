@@ -1,0 +1,359 @@
+#!/usr/bin/env python
+"""Radio hot-path benchmark: CoREAS endpoint field + ZHS vector potential of
+every e+/e- track segment at every antenna, binned into traces, on B200.
+
+Workload (default): 1e7 segments of one seeded synthetic shower at zenith 30 deg
+x 160 antennas (8 arms x 20 radii, 25-500 m), 8192-sample traces at 0.1 ns,
+CoREAS and ZHS fused: 1.6e9 track-antenna pairs per step.  A step is one
+accumulateLeptonTracks over the whole batch (record ingest + projection).
+
+One JSON line on rank 0:
+  value       pairs/s of the production path (windowed, mixed precision) with
+              the records resident in HBM, device time (CUDA events), max over ranks
+  e2e         the same metric through the C ABI with host records: per step
+              reset + enqueueHostLeptonTracks (pinned host -> device) + download
+              (decoded traces device -> host)
+  roofline    FP64 roofline of the projection kernel against the FP64 FMA rate
+              measured on the same GPU in this run
+  cpu_baseline  the reference's own projection code on the host cores
+--impl reference times that CPU implementation alone on a bounded sample.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+from datetime import timedelta
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+import __graft_entry__ as entry  # noqa: E402
+
+# Algorithmic work per unit, counted from the reference's expressions
+# (RadioProjection.inl): FP64 add/sub/mul plus division/sqrt, each one FLOP.
+FLOP_COREAS_PAIR = 108 + 14   # two propagations, two Doppler factors, two fields, two samples
+FLOP_ZHS_SETUP = 40 + 12      # Fraunhofer midpoint propagation and subdivision
+FLOP_ZHS_SUBTRACK = 79 + 7    # one segment: propagation, detection times, potential
+FLOP_SAMPLE = 12 + 3          # bin, gate and three fixed-point conversions
+
+WORKLOAD_NAME = "tiled_c1"
+
+
+def parse_args():
+    p = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--workload", default=WORKLOAD_NAME)
+    p.add_argument("--segments", type=int, default=0, help="override the segment count")
+    p.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
+    p.add_argument("--kernel", choices=["windowed", "direct"], default="windowed")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-baseline", action="store_true")
+    p.add_argument("--no-variants", action="store_true",
+                   help="skip the FP64 windowed and plain FP64 direct comparison runs")
+    p.add_argument("--baseline-segments", type=int, default=100_000)
+    return p.parse_args()
+
+
+def env_rank():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=self.file, stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        self.file.flush()
+        rows = []
+        with open(self.file.name) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.file.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ------------------------------------------------------------------ workload
+def build_workload(name: str, segments: int, seed: int):
+    pkg = entry.load_package()
+    from corsika8_kokkos_b200 import showers
+
+    wl, gen, default_n = showers.workload_config(name)
+    n = segments or default_n
+    if gen.get("ice"):
+        records = showers.ice_records(n, seed=seed, **gen)
+    else:
+        records = showers.shower_records(n, seed=seed, **gen)
+    return pkg, showers, wl, records
+
+
+def algorithmic_flops(pairs: int, counters: dict) -> float:
+    return (pairs * (FLOP_COREAS_PAIR + FLOP_ZHS_SETUP) +
+            counters["zhs_subtracks"] * FLOP_ZHS_SUBTRACK +
+            (counters["coreas_contributions"] + counters["zhs_contributions"]) * FLOP_SAMPLE)
+
+
+# ------------------------------------------------------------------ reference arm
+def cpu_reference_rate(wl, records, showers, threads: int, steps: int = 1, warmup: int = 0):
+    """Times the reference's own projection code (oracle/_ref) on the host cores,
+    or the C restatement of it when the reference library is not built."""
+    oracle = entry.load_oracle()
+    kind = "reference" if oracle.reference_available() else "port"
+    backend = oracle.reference() if kind == "reference" else oracle.restatement()
+    config = showers.make_config(wl)
+    pairs = records.size * len(wl["observers"])
+    for _ in range(warmup):
+        backend.project(config, records, threads=threads)
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        backend.project(config, records, threads=threads)
+        times.append(time.perf_counter() - t0)
+    return pairs, times, kind
+
+
+def run_reference(args):
+    rank, world, _ = env_rank()
+    if rank != 0:
+        return
+    n = args.baseline_segments
+    pkg, showers, wl, records = build_workload(args.workload, n, seed=1000)
+    threads = os.cpu_count() or 1
+    pairs, times, kind = cpu_reference_rate(wl, records, showers, threads, args.steps,
+                                            max(0, min(args.warmup, 1)))
+    seconds = sum(times) / len(times)
+    value = pairs / seconds
+    sample = (f"{n} of the workload's segments x {len(wl['observers'])} antennas "
+              f"({pairs:.3g} pairs) per step, fixed-point CoREAS+ZHS")
+    line = {
+        "impl": "reference", "metric": "track-antenna pairs/s", "value": value,
+        "unit": "pairs/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": seconds * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded shower generator)",
+        "config": {"workload": args.workload, "segments": n,
+                   "antennas": int(len(wl["observers"])),
+                   "bins": int(wl["observers"]["number_of_bins"][0])},
+        "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": threads, "kind": kind,
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ our arm
+def run_ours(args):
+    rank, world, local = env_rank()
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    pkg, showers, wl, records = build_workload(args.workload, args.segments, seed=1000 + rank)
+    n = records.size
+    observers = len(wl["observers"])
+    pairs_per_step = n * observers
+    device_records = torch.from_numpy(records.view(np.uint8).reshape(-1)).cuda()
+    stream = torch.cuda.current_stream()
+    precision = {"mixed": 1, "fp64": 0}[args.precision]
+    kernel = {"windowed": 2, "direct": 1}[args.kernel]
+    peaks = pkg.probe_peaks()
+
+    def timed_run(precision, kernel, steps, warmup, timing=True):
+        config = showers.make_config(wl, precision=precision, kernel=kernel)
+        acc = pkg.RadioAccumulator(config, stream=stream.cuda_stream)
+        ptr = device_records.data_ptr()
+        for _ in range(warmup):
+            acc.accumulate_lepton_tracks(ptr, n)
+        acc.reset()
+        acc.set_kernel_timing(timing)
+        barrier()
+        torch.cuda.synchronize()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(local) as clocks:
+            start.record(stream)
+            for _ in range(steps):
+                acc.accumulate_lepton_tracks(ptr, n)
+            end.record(stream)
+            torch.cuda.synchronize()
+        barrier()
+        ms = start.elapsed_time(end) / steps
+        stats = acc.statistics()
+        kernel_ms = stats.kernel_time_ms / max(stats.timed_launches, 1)
+        counters = acc.download().counters
+        acc.close()
+        return ms, kernel_ms, counters, clocks.summary(), stats
+
+    ms, kernel_ms, counters, clocks, stats = timed_run(precision, kernel, args.steps, args.warmup)
+    ms_max = max_over_ranks(ms)
+    value = world * pairs_per_step / (ms_max * 1e-3)
+
+    variants = {}
+    if not args.no_variants and world == 1:
+        for label, prec, kern, steps in (("fp64_windowed", 0, 2, 2), ("fp64_direct_plain", 0, 1, 1)):
+            if prec == precision and kern == kernel:
+                continue
+            vms, vkms, vcounters, vclocks, _ = timed_run(prec, kern, steps, 1)
+            variants[label] = {"pairs_per_s": pairs_per_step / (vms * 1e-3), "ms_per_step": vms,
+                               "kernel_ms": vkms, "clocks_sm_mhz": vclocks.get("sm_mhz")}
+
+    # roofline of the projection kernel (per launch = per step)
+    flops = algorithmic_flops(pairs_per_step, {k: counters[k] / args.steps for k in
+                                               ("zhs_subtracks", "coreas_contributions",
+                                                "zhs_contributions")})
+    achieved = flops / (kernel_ms * 1e-3) / 1e12
+    peak = peaks["fp64_flops"] / 1e12
+    roofline = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak if peak else None, "traffic": None,
+                "peak_source": "FP64 FMA stream measured in this run (c8r_probe_peaks)",
+                "kernel": "windowed_kernel (projection)", "kernel_ms": kernel_ms,
+                "flop_per_launch": flops,
+                "atomics": {"shared_per_s_peak": peaks["shared_atomics_per_s"],
+                            "global_per_s_peak": peaks["global_atomics_per_s"],
+                            "samples_per_s": (counters["coreas_contributions"] +
+                                              counters["zhs_contributions"]) / args.steps /
+                                             (kernel_ms * 1e-3)}}
+
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(pkg, showers, wl, records, precision, kernel, stream, args, torch, barrier,
+                      max_over_ranks, world)
+
+    baseline = None
+    if rank == 0 and world == 1 and not args.no_baseline:
+        sample = records[: args.baseline_segments]
+        threads = os.cpu_count() or 1
+        bpairs, btimes, kind = cpu_reference_rate(wl, sample, showers, threads, 1, 0)
+        baseline = {"value": bpairs / btimes[0], "unit": "pairs/s", "cores": threads, "kind": kind,
+                    "sample": f"first {sample.size} of {n} segments x {observers} antennas "
+                              f"({bpairs:.3g} pairs), fixed-point CoREAS+ZHS, one pass"}
+
+    if world > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": "track-antenna pairs/s", "value": value, "unit": "pairs/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 times / f32 amplitudes" if precision == 1 else "f64",
+        "data": "synthetic (seeded shower generator, one shower per GPU)",
+        "config": {"workload": args.workload, "segments": n, "antennas": observers,
+                   "bins": int(wl["observers"]["number_of_bins"][0]),
+                   "algorithms": "CoREAS+ZHS fused", "precision": args.precision,
+                   "kernel": args.kernel, "pairs_per_step": pairs_per_step,
+                   "l2": "inputs larger than L2 (7.5 GB records, 1.1 GB kinematics)"},
+        "e2e": e2e, "roofline": roofline, "cpu_baseline": baseline,
+        "clocks": clocks, "gpu_launches": 2 * args.steps,
+        "counters": {k: counters[k] for k in ("valid_tracks", "coreas_contributions",
+                                              "zhs_contributions", "zhs_subtracks",
+                                              "fixed_point_overflows")},
+        "variants": variants, "peaks": peaks,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_e2e(pkg, showers, wl, records, precision, kernel, stream, args, torch, barrier,
+            max_over_ranks, world):
+    """reset + enqueueHostLeptonTracks(pinned host records) + download(pinned traces)."""
+    config = showers.make_config(wl, precision=precision, kernel=kernel)
+    tuning = pkg.TuningParameters(batch_size=1 << 18)
+    acc = pkg.RadioAccumulator(config, tuning, stream=stream.cuda_stream)
+    cudart = torch.cuda.cudart()
+    registered = cudart.cudaHostRegister(records.ctypes.data, records.nbytes, 0) == 0
+    out_c = torch.empty(3 * acc.coreas_bins, dtype=torch.float64, pin_memory=True).numpy()
+    out_z = torch.empty(3 * acc.zhs_bins, dtype=torch.float64, pin_memory=True).numpy()
+    for _ in range(max(1, min(args.warmup, 2))):
+        acc.reset()
+        acc.enqueue_host_lepton_tracks(records)
+        acc.download_into(out_c, out_z)
+    barrier()
+    steps = max(1, min(args.steps, 3))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        acc.reset()
+        acc.enqueue_host_lepton_tracks(records)
+        acc.download_into(out_c, out_z)
+    seconds = (time.perf_counter() - t0) / steps
+    seconds = max_over_ranks(seconds)
+    acc.close()
+    if registered:
+        cudart.cudaHostUnregister(records.ctypes.data)
+    pairs = records.size * len(wl["observers"])
+    return {"value": world * pairs / seconds, "unit": "pairs/s",
+            "h2d_bytes_per_step": int(records.nbytes),
+            "d2h_bytes_per_step": int(out_c.nbytes + out_z.nbytes),
+            "ms_per_step": seconds * 1e3, "pinned_input": bool(registered)}
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

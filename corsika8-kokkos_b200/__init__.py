@@ -183,6 +183,14 @@ class TuningParameters:
                           self.track_tile_size, self.observer_tile_size, self.device_queues)
 
 
+def probe_peaks() -> dict:
+    """FP64/FP32 FMA and 64-bit shared/global atomic rates measured on the current GPU."""
+    lib = library()
+    p = abi.Peaks()
+    _raise(lib.c8r_probe_peaks(C.byref(p)), b"probe failed")
+    return {name: getattr(p, name) for name, _ in abi.Peaks._fields_}
+
+
 def validate(config: RadioConfig) -> None:
     lib = library()
     cfg, keep = config.to_c()
@@ -338,3 +346,6 @@ class RadioAccumulator:
 
     def synchronize(self) -> None:
         self._check(self._lib.c8r_synchronize(self._h))
+
+    def set_kernel_timing(self, enabled: bool) -> None:
+        self._check(self._lib.c8r_set_kernel_timing(self._h, int(enabled)))

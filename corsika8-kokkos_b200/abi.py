@@ -192,8 +192,14 @@ class Statistics(C.Structure):
         ("track_tile_size", C.c_uint32),
         ("observer_tile_size", C.c_uint32),
         ("kernel_time_ms", C.c_double),
+        ("timed_launches", C.c_uint64),
         ("counters", Counters),
     ]
+
+
+class Peaks(C.Structure):
+    _fields_ = [("fp64_flops", C.c_double), ("fp32_flops", C.c_double),
+                ("shared_atomics_per_s", C.c_double), ("global_atomics_per_s", C.c_double)]
 
 
 # Exported symbols of libc8radio.so and their prototypes.
@@ -220,6 +226,8 @@ PROTOTYPES = {
     "c8r_projected_track_capacity": (
         C.c_int, [C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
     "c8r_synchronize": (C.c_int, [C.c_void_p]),
+    "c8r_set_kernel_timing": (C.c_int, [C.c_void_p, C.c_int]),
+    "c8r_probe_peaks": (C.c_int, [C.POINTER(Peaks)]),
 }
 
 

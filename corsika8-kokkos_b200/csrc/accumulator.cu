@@ -202,8 +202,6 @@ class Accumulator {
     staging_.allocate(host_batch_);
     for (auto& h : host_) h.allocate(host_batch_);
     for (auto& e : host_ready_) check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
-    check(cudaEventCreate(&kernel_begin_), "event");
-    check(cudaEventCreate(&kernel_end_), "event");
     fuse_ = coreas_enabled_ && zhs_enabled_ && observers_share_grid();
     initialized_ = true;
     reset();
@@ -211,10 +209,17 @@ class Accumulator {
 
   ~Accumulator() {
     if (stream_ || initialized_) cudaStreamSynchronize(stream_);
+    if (copy_stream_) {
+      cudaStreamSynchronize(copy_stream_);
+      cudaStreamDestroy(copy_stream_);
+    }
+    for (auto& e : copy_done_)
+      if (e) cudaEventDestroy(e);
+    for (auto& e : consumed_)
+      if (e) cudaEventDestroy(e);
     for (auto& e : host_ready_)
       if (e) cudaEventDestroy(e);
-    if (kernel_begin_) cudaEventDestroy(kernel_begin_);
-    if (kernel_end_) cudaEventDestroy(kernel_end_);
+    for (auto e : all_events_) cudaEventDestroy(e);
   }
 
   bool enabled() const { return initialized_ && enabled_; }
@@ -231,6 +236,7 @@ class Accumulator {
     }
     check(cudaMemsetAsync(counters_.ptr, 0, sizeof(DeviceCounters), stream_), "memset");
     check(cudaStreamSynchronize(stream_), "reset fence");
+    resolve_timing();
     stats_ = c8r_statistics{};
     stats_.device_bytes = device_bytes();
     stats_.track_tile_size = static_cast<uint32_t>(chunk_hint());
@@ -244,6 +250,14 @@ class Accumulator {
     if (!enabled()) throw std::logic_error("host radio tracks requested while radio is disabled");
     if (downloaded_ || sealed_) throw std::logic_error("radio already downloaded; reset before host tracks");
     if (count != 0 && records == nullptr) throw std::invalid_argument("null host radio track input");
+    if (count >= host_batch_ && host_count_ == 0 && is_pinned(records)) {
+      // Page-locked caller memory: DMA whole batches straight from it, then
+      // wait for the copies before returning (the caller may reuse it).
+      std::size_t const whole = count - count % host_batch_;
+      enqueue_pinned(records, whole);
+      records += whole;
+      count -= whole;
+    }
     while (count != 0) {
       if (host_count_ == 0) check(cudaEventSynchronize(host_ready_[host_index_]), "staging wait");
       std::size_t const copied = std::min(count, host_batch_ - host_count_);
@@ -254,6 +268,48 @@ class Accumulator {
       count -= copied;
       if (host_count_ == host_batch_) flush();
     }
+  }
+
+  static bool is_pinned(void const* p) {
+    cudaPointerAttributes attributes{};
+    if (cudaPointerGetAttributes(&attributes, p) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    return attributes.type == cudaMemoryTypeHost;
+  }
+
+  // Batches of host_batch_ records copied from pinned caller memory into a
+  // pair of device staging buffers (copy of batch k+1 overlaps projection of
+  // batch k on the copy stream); returns after the last copy completed.
+  void enqueue_pinned(c8r_lepton_transport_record const* records, std::size_t count) {
+    if (!copy_stream_) {
+      check(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking), "copy stream");
+      for (auto& e : copy_done_) check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+      for (auto& e : consumed_) check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+      staging2_.allocate(host_batch_);
+    }
+    // earlier work on the accumulator stream may still read staging_
+    for (auto& e : consumed_) check(cudaEventRecord(e, stream_), "event");
+    std::size_t const batches = count / host_batch_;
+    for (std::size_t b = 0; b < batches; ++b) {
+      int const k = static_cast<int>(b & 1);
+      c8r_lepton_transport_record* dst = k ? staging2_.ptr : staging_.ptr;
+      // the staging buffer is free once the ingest that read it has run
+      check(cudaStreamWaitEvent(copy_stream_, consumed_[k], 0), "wait");
+      check(cudaMemcpyAsync(dst, records + b * host_batch_,
+                            host_batch_ * sizeof(c8r_lepton_transport_record),
+                            cudaMemcpyHostToDevice, copy_stream_),
+            "host track upload");
+      check(cudaEventRecord(copy_done_[k], copy_stream_), "event");
+      check(cudaStreamWaitEvent(stream_, copy_done_[k], 0), "wait");
+      accumulate_device(dst, host_batch_, host_batch_);
+      check(cudaEventRecord(consumed_[k], stream_), "event");
+      stats_.host_to_device_bytes += host_batch_ * sizeof(c8r_lepton_transport_record);
+      ++stats_.host_track_batches;
+      stats_.host_tracks_enqueued += host_batch_;
+    }
+    check(cudaStreamSynchronize(copy_stream_), "host track upload");
   }
 
   // RadioAccumulator::flushHostLeptonTracks, RadioAccumulator.inl:274-290.  The
@@ -288,7 +344,11 @@ class Accumulator {
     ++stats_.track_precompute_batches;
     stats_.track_precomputed_records += count;
     stats_.maximum_track_batch = std::max<uint64_t>(stats_.maximum_track_batch, count);
-    if (timing_) check(cudaEventRecord(kernel_begin_, stream_), "event");
+    cudaEvent_t begin = nullptr, end = nullptr;
+    if (timing_) {
+      begin = timing_event();
+      check(cudaEventRecord(begin, stream_), "event");
+    }
     bool const direct = kernel_ == C8R_KERNEL_DIRECT ||
                         (kernel_ == C8R_KERNEL_AUTO && count < kDirectThreshold);
     if (direct)
@@ -296,13 +356,25 @@ class Accumulator {
     else
       project_windowed(count);
     if (timing_) {
-      check(cudaEventRecord(kernel_end_, stream_), "event");
-      check(cudaEventSynchronize(kernel_end_), "event");
-      float ms = 0.f;
-      check(cudaEventElapsedTime(&ms, kernel_begin_, kernel_end_), "event time");
-      stats_.kernel_time_ms += ms;
+      end = timing_event();
+      check(cudaEventRecord(end, stream_), "event");
+      pending_.push_back({begin, end});
     }
     downloaded_ = false;
+  }
+
+  // Sums the projection-kernel time of completed launches (blocks on them).
+  void resolve_timing() {
+    for (auto const& p : pending_) {
+      check(cudaEventSynchronize(p.second), "event");
+      float ms = 0.f;
+      check(cudaEventElapsedTime(&ms, p.first, p.second), "event time");
+      stats_.kernel_time_ms += ms;
+      ++stats_.timed_launches;
+      free_events_.push_back(p.first);
+      free_events_.push_back(p.second);
+    }
+    pending_.clear();
   }
 
   // RadioAccumulator::download, RadioAccumulator.inl:407-439 (decode on the device).
@@ -365,11 +437,14 @@ class Accumulator {
     downloaded_ = true;
   }
 
-  void statistics(c8r_statistics& out) const { out = stats_; }
+  void statistics(c8r_statistics& out) {
+    resolve_timing();
+    out = stats_;
+  }
 
   std::size_t device_bytes() const {
     std::size_t total = table_.bytes() + counters_.bytes() + slot_.bytes() + next_item_.bytes() +
-                        staging_.bytes() + tracks_.bytes();
+                        staging_.bytes() + staging2_.bytes() + tracks_.bytes();
     for (int a = 0; a < 2; ++a)
       total += observers_[a].bytes() + fixed_traces_[a].bytes() + float_traces_[a].bytes() +
                decoded_[a].bytes() + decode_offsets_[a].bytes() + decode_factors_[a].bytes();
@@ -402,6 +477,18 @@ class Accumulator {
 
   std::size_t bins(int a) const { return bins_[a]; }
   void set_timing(bool on) { timing_ = on; }
+
+  cudaEvent_t timing_event() {
+    if (!free_events_.empty()) {
+      cudaEvent_t e = free_events_.back();
+      free_events_.pop_back();
+      return e;
+    }
+    cudaEvent_t e = nullptr;
+    check(cudaEventCreate(&e), "event");
+    all_events_.push_back(e);
+    return e;
+  }
 
   // Work-plan access for the batched launcher.
   EventPlan event_plan(std::size_t count) const { return make_event(count); }
@@ -678,10 +765,14 @@ class Accumulator {
   DeviceBuffer<unsigned> next_item_;
   DeviceBuffer<double> tracks_;
   std::size_t capacity_ = 0;
-  DeviceBuffer<c8r_lepton_transport_record> staging_;
+  DeviceBuffer<c8r_lepton_transport_record> staging_, staging2_;
+  cudaStream_t copy_stream_ = nullptr;
+  cudaEvent_t copy_done_[2] = {nullptr, nullptr};
+  cudaEvent_t consumed_[2] = {nullptr, nullptr};
   PinnedBuffer<c8r_lepton_transport_record> host_[2];
   cudaEvent_t host_ready_[2] = {nullptr, nullptr};
-  cudaEvent_t kernel_begin_ = nullptr, kernel_end_ = nullptr;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending_;
+  std::vector<cudaEvent_t> free_events_, all_events_;
   int host_index_ = 0;
   std::size_t host_count_ = 0;
   std::size_t host_batch_ = kDefaultHostBatch;
@@ -847,8 +938,8 @@ int c8r_total_bins(const c8r_accumulator* handle, size_t* coreas_bins, size_t* z
 int c8r_get_statistics(const c8r_accumulator* handle, c8r_statistics* statistics) {
   if (int s = with_handle(handle, nullptr, true)) return s;
   if (!statistics) return C8R_INVALID_ARGUMENT;
-  handle->impl->statistics(*statistics);
-  return C8R_OK;
+  auto* h = const_cast<c8r_accumulator*>(handle);
+  return guarded(&h->error, [&] { h->impl->statistics(*statistics); });
 }
 
 int c8r_device_bytes(const c8r_accumulator* handle, size_t* bytes) {
@@ -879,6 +970,12 @@ int c8r_projected_track_capacity(const c8r_accumulator* handle, size_t count,
   if (retained_bytes) *retained_bytes = r;
   if (transient_peak_bytes) *transient_peak_bytes = p;
   return status;
+}
+
+int c8r_set_kernel_timing(c8r_accumulator* handle, int enabled) {
+  if (int s = with_handle(handle, nullptr, true)) return s;
+  handle->impl->set_timing(enabled != 0);
+  return C8R_OK;
 }
 
 int c8r_synchronize(c8r_accumulator* handle) {

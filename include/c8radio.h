@@ -187,9 +187,18 @@ typedef struct c8r_statistics {
   uint64_t maximum_track_batch;
   uint32_t track_tile_size;
   uint32_t observer_tile_size;
-  double kernel_time_ms;      /* CUDA-event time of projection kernels (if timing on) */
+  double kernel_time_ms;      /* CUDA-event time of projection kernels (timing on) */
+  uint64_t timed_launches;    /* projection launches included in kernel_time_ms */
   c8r_counters counters;      /* last downloaded device counters */
 } c8r_statistics;
+
+/* Measured device rates used as roofline denominators (c8r_probe_peaks). */
+typedef struct c8r_peaks {
+  double fp64_flops;            /* FP64 FMA stream, 2 FLOP per FMA */
+  double fp32_flops;            /* FP32 FMA stream, 2 FLOP per FMA */
+  double shared_atomics_per_s;  /* 64-bit shared-memory atomic adds, distinct addresses */
+  double global_atomics_per_s;  /* 64-bit global atomic adds over 128 MiB */
+} c8r_peaks;
 
 typedef struct c8r_accumulator c8r_accumulator;
 
@@ -217,7 +226,9 @@ int c8r_enabled(const c8r_accumulator* handle, int* enabled);
 /* RadioAccumulator::reset (RadioAccumulator.inl:224-250). */
 int c8r_reset(c8r_accumulator* handle);
 /* RadioAccumulator::enqueueHostLeptonTracks (RadioAccumulator.inl:252-272):
- * copies before returning; full 4096-record batches are flushed. */
+ * copies before returning; full batches (tuning batch_size, default 4096
+ * records) are flushed.  Page-locked input is copied by DMA straight into
+ * device staging (the call returns once those copies completed). */
 int c8r_enqueue_host(c8r_accumulator* handle, const c8r_lepton_transport_record* records,
                      size_t count);
 /* RadioAccumulator::flushHostLeptonTracks (RadioAccumulator.inl:274-290). */
@@ -250,6 +261,13 @@ int c8r_static_host_to_device_bytes(const c8r_accumulator* handle, size_t* bytes
 int c8r_reserve(c8r_accumulator* handle, size_t count);
 int c8r_projected_track_capacity(const c8r_accumulator* handle, size_t count,
                                  size_t* retained_bytes, size_t* transient_peak_bytes);
+/* B200 extension: when enabled, each accumulate records CUDA events around
+ * its projection kernels (no host synchronisation); c8r_get_statistics sums
+ * the elapsed times of completed launches into kernel_time_ms. */
+int c8r_set_kernel_timing(c8r_accumulator* handle, int enabled);
+/* B200 extension, no reference counterpart: measures the rates of c8r_peaks
+ * on the current device (a few milliseconds of probe kernels). */
+int c8r_probe_peaks(c8r_peaks* peaks);
 /* Blocks until all work queued on the accumulator's stream has completed. */
 int c8r_synchronize(c8r_accumulator* handle);
 

@@ -1,0 +1,256 @@
+"""GPU parity: the sm_100a kernels through the C ABI against the oracle.
+
+Fixed-point (deterministic) traces are compared bit for bit; floating traces
+(FP64 atomics, order-dependent) within 1e-12 of each trace's peak; the mixed
+path within 1e-4 relative L2 per trace with identical contribution counters.
+"""
+import numpy as np
+import pytest
+
+import cases
+
+pytestmark = pytest.mark.gpu
+
+KERNELS = {"direct": 1, "windowed": 2}
+EXACT_COUNTERS = ("coreas_contributions", "zhs_contributions", "zhs_subtracks", "valid_tracks",
+                  "fixed_point_overflows")
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+
+    assert torch.cuda.is_available(), "GPU tests need CUDA"
+    return torch
+
+
+def to_device(torch, records):
+    return torch.from_numpy(np.ascontiguousarray(records).view(np.uint8).reshape(-1)).cuda()
+
+
+def gpu_project(pkg, torch, config, records, kernel=None, tuning=None):
+    if kernel is not None:
+        config.kernel = kernel
+    acc = pkg.RadioAccumulator(config, tuning)
+    raw = to_device(torch, records) if records.size else None
+    if records.size:
+        acc.accumulate_lepton_tracks(raw.data_ptr(), records.size)
+    if config.deterministic:
+        coreas, zhs, counters = acc.download_fixed()
+    else:
+        w = acc.download()
+        coreas, zhs, counters = w.coreas, w.zhs, w.counters
+    stats = acc.statistics()
+    acc.close()
+    return coreas, zhs, counters, stats
+
+
+def assert_same(got, want, deterministic):
+    for g, w in ((got[0], want[0]), (got[1], want[1])):
+        assert g.shape == w.shape
+        if deterministic:
+            assert np.array_equal(g, w), f"{np.count_nonzero(g != w)} of {g.size} values differ"
+        else:
+            peak = max(np.abs(w).max(initial=0.0), 1e-300)
+            assert np.abs(g - w).max(initial=0.0) <= 1e-28 + 2e-12 * peak
+    for key in EXACT_COUNTERS:
+        assert got[2][key] == want[2][key], key
+
+
+@pytest.mark.parametrize("kernel", list(KERNELS))
+def test_scalar_cases(pkg, oracle, torch_cuda, kernel):
+    for name, config, record in cases.scalar_cases():
+        for integer in (False, True):
+            for mode in (1, 2, 3):
+                config.deterministic = integer
+                config.coreas_enabled = bool(mode & 1)
+                config.zhs_enabled = bool(mode & 2)
+                want = oracle.restatement().project(config, record, threads=1)
+                got = gpu_project(pkg, torch_cuda, config, record, KERNELS[kernel])
+                assert_same(got, want, integer)
+
+
+@pytest.mark.parametrize("kernel", list(KERNELS))
+def test_homogeneous_refinement_and_invalid(pkg, oracle, torch_cuda, kernel):
+    name, config, record = cases.scalar_cases()[0]
+    for index in (1.0, 1.0003, 1.78):
+        config.propagation.homogeneous_refractive_index = index
+        config.zhs_subtrack_refinement = 3
+        want = oracle.restatement().project(config, record, threads=1)
+        assert_same(gpu_project(pkg, torch_cuda, config, record, KERNELS[kernel]), want, True)
+    invalid = cases.invalid_records(record)
+    got = gpu_project(pkg, torch_cuda, config, invalid, KERNELS[kernel])
+    assert got[2]["valid_tracks"] == 0
+    assert not got[0].any() and not got[1].any()
+
+
+@pytest.mark.parametrize("kernel", list(KERNELS))
+def test_accumulator_grid(pkg, oracle, torch_cuda, kernel):
+    for label, config, count in cases.accumulator_grid():
+        records = cases.accumulator_tracks(count)
+        want = oracle.restatement().project(config, records, threads=8)
+        got = gpu_project(pkg, torch_cuda, config, records, KERNELS[kernel])
+        assert_same(got, want, config.deterministic)
+        if config.track_diagnostics:
+            for key in ("weighted_segment_count", "track_length_m", "weighted_track_length_m",
+                        "energy_weighted_track_length_gev_m", "maximum_segment_length_m",
+                        "weighted_beta_deficit_track_length_m", "weighted_time_residual_s"):
+                np.testing.assert_allclose(got[2][key], want[2][key], rtol=1e-12, atol=1e-30)
+            np.testing.assert_allclose(got[2]["weighted_track_length_by_kinetic_energy_m"],
+                                       want[2]["weighted_track_length_by_kinetic_energy_m"],
+                                       rtol=1e-12, atol=1e-30)
+
+
+def _workload_records(showers, name, count, seed):
+    wl, gen, _ = showers.workload_config(name)
+    if gen.get("ice"):
+        return wl, showers.ice_records(count, seed=seed, **gen)
+    return wl, showers.shower_records(count, seed=seed, **gen)
+
+
+@pytest.mark.parametrize("name,count", [("plain_c0", 100_000), ("tiled_c1", 20_000),
+                                        ("ice_c2", 50_000)])
+@pytest.mark.parametrize("kernel", list(KERNELS))
+def test_synthetic_showers_bit_exact(pkg, oracle, showers, torch_cuda, name, count, kernel):
+    wl, records = _workload_records(showers, name, count, seed=21)
+    config = showers.make_config(wl)
+    want = oracle.restatement().project(config, records, threads=16)
+    got = gpu_project(pkg, torch_cuda, config, records, KERNELS[kernel])
+    assert_same(got, want, True)
+    assert got[2]["coreas_contributions"] > 0 and got[2]["zhs_contributions"] > 0
+
+
+def relative_l2_per_trace(got, want, observers):
+    errors = []
+    offset = 0
+    for n in observers["number_of_bins"]:
+        n = int(n)
+        g, w = got[:, offset:offset + n], want[:, offset:offset + n]
+        norm = np.linalg.norm(w)
+        if norm > 0:
+            errors.append(np.linalg.norm(g - w) / norm)
+        offset += n
+    return np.array(errors)
+
+
+@pytest.mark.parametrize("name,count", [("plain_c0", 100_000), ("tiled_c1", 20_000),
+                                        ("ice_c2", 50_000)])
+def test_mixed_precision_within_1e4(pkg, oracle, showers, torch_cuda, name, count):
+    wl, records = _workload_records(showers, name, count, seed=33)
+    exact_cfg = showers.make_config(wl)
+    want = oracle.restatement().project(exact_cfg, records, threads=16)
+    scale = exact_cfg.fixed_point_field_limit_v_per_m / 2.0 ** 62
+    fs = wl["observers"]["sample_rate_hz"][0]
+    for kernel in KERNELS.values():
+        mixed = showers.make_config(wl, precision=1, kernel=kernel)
+        got = gpu_project(pkg, torch_cuda, mixed, records)
+        for key in ("coreas_contributions", "zhs_contributions", "zhs_subtracks", "valid_tracks"):
+            assert got[2][key] == want[2][key], key
+        for a, factor in ((0, 1.0), (1, fs)):
+            err = relative_l2_per_trace(got[a] * (scale / factor), want[a] * (scale / factor),
+                                        wl["observers"])
+            assert err.max() <= 1e-4, (a, err.max())
+
+
+def test_host_enqueue_batches_match_device_path(pkg, oracle, showers, torch_cuda):
+    """Bounded-batch host replay equals the device path (testRadioSpoolReplay.cpp:37-112)."""
+    wl, records = _workload_records(showers, "plain_c0", 9000, seed=5)
+    config = showers.make_config(wl)
+    want = oracle.restatement().project(config, records, threads=8)
+    for batch in (1, 7, 4096, 65536):
+        acc = pkg.RadioAccumulator(config, pkg.TuningParameters(batch_size=batch))
+        pieces = np.array_split(records, 5) if batch > 1 else [records[:300]]
+        expected = want if batch > 1 else oracle.restatement().project(config, records[:300], threads=4)
+        for piece in pieces:
+            acc.enqueue_host_lepton_tracks(piece)
+        coreas, zhs, counters = acc.download_fixed()
+        stats = acc.statistics()
+        acc.close()
+        assert_same((coreas, zhs, counters), expected, True)
+        assert stats.host_tracks_enqueued == sum(p.size for p in pieces)
+
+
+def test_lifecycle_contracts(pkg, showers, torch_cuda):
+    """Rejection contracts of testRadioAccumulator.cpp:216-302."""
+    wl, records = _workload_records(showers, "plain_c0", 100, seed=1)
+    config = showers.make_config(wl)
+    acc = pkg.RadioAccumulator(config)
+    raw = to_device(torch_cuda, records)
+    with pytest.raises(pkg.OutOfRange):
+        acc.accumulate_lepton_tracks(raw.data_ptr(), 10, extent=5)
+    with pytest.raises(pkg.InvalidArgument):
+        acc.enqueue_host_pointer(None, 1)
+    acc.enqueue_host_pointer(None, 0)
+    acc.enqueue_host_lepton_tracks(records[:1])
+    with pytest.raises(pkg.LogicError):
+        acc.reset()
+    first = acc.download()
+    with pytest.raises(pkg.LogicError):
+        acc.download()
+    with pytest.raises(pkg.LogicError):
+        acc.enqueue_host_lepton_tracks(records[:1])
+    acc.reset()
+    empty = acc.download()
+    assert not empty.coreas.any() and not empty.zhs.any()
+    acc.reset()
+    acc.enqueue_host_lepton_tracks(records[:1])
+    again = acc.download()
+    assert np.array_equal(first.coreas, again.coreas) and np.array_equal(first.zhs, again.zhs)
+    acc.close()
+    off = pkg.RadioAccumulator(pkg.RadioConfig(enabled=False))
+    assert not off.enabled()
+    assert off.download().coreas.size == 0
+    off.close()
+    for variant in range(7):
+        bad = showers.make_config(wl)
+        bad.coreas_observers = bad.coreas_observers.copy()
+        bad.zhs_observers = bad.zhs_observers.copy()
+        if variant == 0:
+            bad.coreas_enabled = bad.zhs_enabled = False
+        elif variant == 1:
+            bad.fixed_point_field_limit_v_per_m = 0.0
+        elif variant == 2:
+            bad.zhs_subtrack_refinement = 0
+        elif variant == 3:
+            bad.zhs_subtrack_refinement = 65
+        elif variant == 4:
+            bad.coreas_observers[0]["number_of_bins"] = 0
+        elif variant == 5:
+            bad.zhs_observers[0]["sample_rate_hz"] = -1.0
+        else:
+            bad.coreas_observers[0]["position_m"][0] = np.inf
+        with pytest.raises(pkg.InvalidArgument):
+            pkg.projected_device_bytes(bad)
+        with pytest.raises(pkg.InvalidArgument):
+            pkg.RadioAccumulator(bad)
+    with pytest.raises(pkg.InvalidArgument):
+        pkg.RadioAccumulator(config, pkg.TuningParameters(team_size=1025))
+
+
+@pytest.mark.parametrize("kernel", list(KERNELS))
+def test_fixed_point_overflow_is_reported(pkg, showers, torch_cuda, kernel):
+    wl, records = _workload_records(showers, "plain_c0", 3000, seed=9)
+    config = showers.make_config(wl, kernel=KERNELS[kernel])
+    config.fixed_point_field_limit_v_per_m = 1e-30
+    acc = pkg.RadioAccumulator(config)
+    raw = to_device(torch_cuda, records)
+    acc.accumulate_lepton_tracks(raw.data_ptr(), records.size)
+    with pytest.raises(pkg.FixedPointOverflow):
+        acc.download()
+    assert acc.statistics().fixed_point_overflows > 0
+    acc.close()
+
+
+def test_empty_and_repeated_batches(pkg, oracle, showers, torch_cuda):
+    wl, records = _workload_records(showers, "plain_c0", 40_000, seed=4)
+    config = showers.make_config(wl, kernel=2)
+    acc = pkg.RadioAccumulator(config)
+    raw = to_device(torch_cuda, records)
+    acc.accumulate_lepton_tracks(raw.data_ptr(), 0)
+    half = records.size // 2
+    acc.accumulate_lepton_tracks(raw.data_ptr(), half)
+    acc.accumulate_lepton_tracks(raw.data_ptr() + half * records.itemsize, records.size - half)
+    coreas, zhs, counters = acc.download_fixed()
+    acc.close()
+    want = oracle.restatement().project(config, records, threads=16)
+    assert_same((coreas, zhs, counters), want, True)
