@@ -254,3 +254,22 @@ def test_empty_and_repeated_batches(pkg, oracle, showers, torch_cuda):
     acc.close()
     want = oracle.restatement().project(config, records, threads=16)
     assert_same((coreas, zhs, counters), want, True)
+
+
+@pytest.mark.parametrize("kernel", list(KERNELS))
+def test_gpu_reproduces_reference_digests(pkg, torch_cuda, kernel):
+    """Digests of the reference's own fixed-point output, committed in tests/golden."""
+    import importlib.util
+    import json
+    from pathlib import Path
+
+    here = Path(__file__).resolve().parent / "golden"
+    spec = importlib.util.spec_from_file_location("make_golden", here / "make_golden.py")
+    golden = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(golden)
+    expected = json.loads((here / "reference_digests.json").read_text())
+    for label, config, records in golden.golden_cases():
+        coreas, zhs, counters, _ = gpu_project(pkg, torch_cuda, config, records, KERNELS[kernel])
+        assert golden.digest(coreas, zhs) == expected[label]["sha256"], label
+        for key in golden.COUNTERS:
+            assert counters[key] == expected[label][key], (label, key)

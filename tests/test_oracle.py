@@ -214,3 +214,26 @@ def test_threaded_oracle_is_order_independent(oracle, showers):
     one = oracle.restatement().project(config, records, threads=1)
     many = oracle.restatement().project(config, records, threads=8)
     assert np.array_equal(one[0], many[0]) and np.array_equal(one[1], many[1])
+
+
+def test_restatement_reproduces_reference_digests(oracle):
+    """The committed digests were made by the reference's own code (tests/golden/make_golden.py)."""
+    import json
+    from pathlib import Path
+
+    sys_path = Path(__file__).resolve().parent / "golden"
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("make_golden", sys_path / "make_golden.py")
+    golden = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(golden)
+    expected = json.loads((sys_path / "reference_digests.json").read_text())
+    seen = 0
+    for label, config, records in golden.golden_cases():
+        coreas, zhs, counters = oracle.restatement().project(config, records, threads=2)
+        want = expected[label]
+        assert golden.digest(coreas, zhs) == want["sha256"], label
+        for key in golden.COUNTERS:
+            assert counters[key] == want[key], (label, key)
+        seen += 1
+    assert seen == len(expected) == 62
