@@ -168,6 +168,39 @@ __device__ __forceinline__ void add_sample(ObserverCache const& o, Sink& sink, d
   ++contributions;
 }
 
+// A deposit at a bin already known to lie in [0, bins).
+template <bool kFixed, class Amp, class Sink>
+__device__ __forceinline__ void deposit_bin(Sink& sink, uint64_t bin, Deposit<Amp> const& d,
+                                            unsigned long long& contributions,
+                                            unsigned long long& overflows) {
+  if (kFixed) {
+    bool const ax = d.okx && sink.add(0, bin, d.ix);
+    bool const ay = d.oky && sink.add(1, bin, d.iy);
+    bool const az = d.okz && sink.add(2, bin, d.iz);
+    if (!(ax && ay && az)) {
+      ++overflows;
+      return;
+    }
+  } else {
+    sink.addf(0, bin, static_cast<double>(d.value.x));
+    sink.addf(1, bin, static_cast<double>(d.value.y));
+    sink.addf(2, bin, static_cast<double>(d.value.z));
+  }
+  ++contributions;
+}
+
+// One run of consecutive ZHS bins with a common value, left for the warp to
+// deposit cooperatively (count == 0: none).  Values are the fixed-point
+// integers, or the FP64 bit patterns in floating mode.
+struct PendingRange {
+  uint64_t bin;
+  uint32_t count;
+  long long v[3];
+};
+
+// Runs shorter than this are deposited by their own lane.
+constexpr uint32_t kCooperativeRun = 6;
+
 // ---------------------------------------------------------------- CoREAS
 // accumulate_co_reas, RadioProjection.inl:339-409.
 template <bool kFixed, class Amp, class Sink>
@@ -235,12 +268,19 @@ __device__ __forceinline__ void coreas_pair(Track const& t, Propagation const& p
 
 // ---------------------------------------------------------------- ZHS
 // accumulate_zhs_segment, RadioProjection.inl:412-480.
-template <bool kFixed, class Amp, class Sink>
+//
+// kRuns = true (windowed kernel): the intermediate bins of a segment are the
+// consecutive bins nearest(x1) + i whenever x1 lies farther than a rounding
+// bound from a half bin (checked below); they are then deposited as one run,
+// without the per-index division, and long runs are handed to the warp via
+// `pending`.  Otherwise, and always for kRuns = false (the reference-shaped
+// direct kernel), each index is binned by the reference's own expression.
+template <bool kFixed, bool kRuns, class Amp, class Sink>
 __device__ __forceinline__ void zhs_segment(double p1x, double p1y, double p1z, double p2x,
                                             double p2y, double p2z, double t1, double t2,
                                             Track const& t, Propagation const& p,
                                             ObserverCache const& o, Sink& sink, Counts& c,
-                                            bool subdivided) {
+                                            bool subdivided, PendingRange* pending) {
   double const mx = (p1x + p2x) * 0.5, my = (p1y + p2y) * 0.5, mz = (p1z + p2z) * 0.5;
   Path const path = propagate<true>(p, o, mx, my, mz);
   double const bk = t.bx * path.kx + t.by * path.ky + t.bz * path.kz;
@@ -288,6 +328,50 @@ __device__ __forceinline__ void zhs_segment(double p1x, double p1y, double p1z, 
     double const mc = (subdivided ? 1. : sign) * t.constant;
     Deposit<Amp> const mid =
         make_deposit<kFixed>(o, scaled(perp, amp_div(static_cast<Amp>(mc), static_cast<Amp>(dd))));
+    bool binned = false;
+    if (kRuns) {
+      // Index i is binned at y_i = RN(RN(RN(d1 + RN(i/fs)) - t0) fs).  With
+      // u = 2^-53, |y_i - (x1 + i)| <= 6 u M (1 + u)^4 < 2^-50 M for
+      // M = |x1| + i + |d1 fs| + |t0 fs| + 2 (each of the four roundings, and
+      // the two of x1, contribute at most u times a term bounded by M).  The
+      // nearest bin changes only at half-integers, which sit at integer
+      // offsets from each other, so if x1 is farther than that bound from a
+      // half-integer, nearest(y_i) = nearest(x1) + i for every i < nb.
+      double const mag = fabs(x1) + static_cast<double>(nb) + fabs(d1 * fs) +
+                         fabs(o.start_time * fs) + 2.;
+      double const fl = floor(x1);
+      double const f = x1 - fl;
+      if (mag < 0x1p50 && fabs(f - 0.5) > mag * 0x1p-48) {
+        long long const b1 = static_cast<long long>(fl) + (f >= 0.5 ? 1 : 0);
+        long long lo = 1, hi = nb;
+        if (-b1 > lo) lo = -b1;
+        long long const top = static_cast<long long>(o.bins) - b1;
+        if (top < hi) hi = top;
+        if (hi > lo) {
+          uint64_t const first = static_cast<uint64_t>(b1 + lo);
+          uint32_t const count = static_cast<uint32_t>(hi - lo);
+          bool const all_ok = !kFixed || (mid.okx && mid.oky && mid.okz);
+          if (pending && all_ok && count >= kCooperativeRun && pending->count == 0) {
+            pending->bin = first;
+            pending->count = count;
+            if (kFixed) {
+              pending->v[0] = mid.ix;
+              pending->v[1] = mid.iy;
+              pending->v[2] = mid.iz;
+            } else {
+              pending->v[0] = __double_as_longlong(static_cast<double>(mid.value.x));
+              pending->v[1] = __double_as_longlong(static_cast<double>(mid.value.y));
+              pending->v[2] = __double_as_longlong(static_cast<double>(mid.value.z));
+            }
+          } else {
+            for (uint32_t k = 0; k < count; ++k)
+              deposit_bin<kFixed>(sink, first + k, mid, c.zhs, c.overflows);
+          }
+        }
+        binned = true;
+      }
+    }
+    if (!binned) {
     // Samples of index i land in bin nearest((d1 + i/fs - t0) fs), monotone in i
     // and within a hundredth of a bin of x1 + i while all magnitudes stay below
     // 2^40 bins; indices whose bin is surely outside [0, bins) are skipped,
@@ -304,6 +388,7 @@ __device__ __forceinline__ void zhs_segment(double p1x, double p1y, double p1z, 
     }
     for (int index = lo; index < hi; ++index)
       deposit<true, kFixed>(o, sink, d1 + static_cast<double>(index) / fs, mid, c.zhs, c.overflows);
+    }
   }
   frac = fabs(x2 + 0.5 - eb);
   add_sample<true, kFixed>(o, sink, d2,
@@ -312,9 +397,10 @@ __device__ __forceinline__ void zhs_segment(double p1x, double p1y, double p1z, 
 }
 
 // accumulate_zhs, RadioProjection.inl:483-529.
-template <bool kFixed, class Amp, class Sink>
+template <bool kFixed, bool kRuns, class Amp, class Sink>
 __device__ __forceinline__ void zhs_pair(Track const& t, Propagation const& p,
-                                         ObserverCache const& o, Sink& sink, Counts& c) {
+                                         ObserverCache const& o, Sink& sink, Counts& c,
+                                         PendingRange* pending) {
   double const mx = (t.sx + t.ex) * 0.5, my = (t.sy + t.ey) * 0.5, mz = (t.sz + t.ez) * 0.5;
   Path const pm = propagate<false>(p, o, mx, my, mz);
   double const uk = (t.bx * pm.kx + t.by * pm.ky + t.bz * pm.kz) / t.beta_module;
@@ -330,9 +416,9 @@ __device__ __forceinline__ void zhs_pair(Track const& t, Propagation const& p,
   int const refinement = static_cast<int>(p.refinement);
   if (subtracks == 1 && refinement == 1) {
     // divisor is exactly 1: point2 = start + (end - start), time2 likewise
-    zhs_segment<kFixed, Amp>(t.sx, t.sy, t.sz, t.sx + (t.ex - t.sx), t.sy + (t.ey - t.sy),
-                             t.sz + (t.ez - t.sz), t.ts, t.ts + (t.te - t.ts), t, p, o, sink, c,
-                             false);
+    zhs_segment<kFixed, kRuns, Amp>(t.sx, t.sy, t.sz, t.sx + (t.ex - t.sx),
+                                    t.sy + (t.ey - t.sy), t.sz + (t.ez - t.sz), t.ts,
+                                    t.ts + (t.te - t.ts), t, p, o, sink, c, false, pending);
     return;
   }
   double const rd = static_cast<double>(refinement);
@@ -344,7 +430,8 @@ __device__ __forceinline__ void zhs_pair(Track const& t, Propagation const& p,
   for (int index = 0; index < subtracks; ++index) {
     for (int r = 0; r < refinement; ++r) {
       double const p2x = p1x + rx, p2y = p1y + ry, p2z = p1z + rz, t2 = t1 + rt;
-      zhs_segment<kFixed, Amp>(p1x, p1y, p1z, p2x, p2y, p2z, t1, t2, t, p, o, sink, c, true);
+      zhs_segment<kFixed, kRuns, Amp>(p1x, p1y, p1z, p2x, p2y, p2z, t1, t2, t, p, o, sink, c,
+                                      true, pending);
       p1x = p2x;
       p1y = p2y;
       p1z = p2z;
@@ -599,7 +686,7 @@ __global__ void __launch_bounds__(256) direct_kernel(EventPlan ev) {
         sink.row[r] = kFixed ? ev.fixed[1] + r * ev.total_bins[1] + o.offset : nullptr;
         sink.frow[r] = kFixed ? nullptr : ev.floating[1] + r * ev.total_bins[1] + o.offset;
       }
-      zhs_pair<kFixed, Amp>(t, ev.propagation, o, sink, c);
+      zhs_pair<kFixed, false, Amp>(t, ev.propagation, o, sink, c, nullptr);
     }
   }
   flush_counts(c, ev.counters);
@@ -607,6 +694,40 @@ __global__ void __launch_bounds__(256) direct_kernel(EventPlan ev) {
 
 // ---------------------------------------------------------------- windowed
 constexpr int kWindowThreadsMax = 512;
+
+// Each lane's pending run of consecutive ZHS bins is deposited by the whole
+// warp, 32 bins per step.  Every lane of the warp must call it.
+template <bool kFixed, class Sink>
+__device__ __forceinline__ void deposit_runs(Sink& sink, PendingRange const& run, Counts& c) {
+  unsigned mask = __ballot_sync(0xffffffffu, run.count != 0);
+  unsigned const lane = threadIdx.x & 31u;
+  while (mask) {
+    int const src = __ffs(mask) - 1;
+    mask &= mask - 1;
+    uint64_t const first = __shfl_sync(0xffffffffu, run.bin, src);
+    uint32_t const count = __shfl_sync(0xffffffffu, run.count, src);
+    long long const vx = __shfl_sync(0xffffffffu, run.v[0], src);
+    long long const vy = __shfl_sync(0xffffffffu, run.v[1], src);
+    long long const vz = __shfl_sync(0xffffffffu, run.v[2], src);
+    for (uint32_t k = lane; k < count; k += 32u) {
+      uint64_t const bin = first + k;
+      if (kFixed) {
+        bool const ax = sink.add(0, bin, vx);
+        bool const ay = sink.add(1, bin, vy);
+        bool const az = sink.add(2, bin, vz);
+        if (ax && ay && az)
+          ++c.zhs;
+        else
+          ++c.overflows;
+      } else {
+        sink.addf(0, bin, __longlong_as_double(vx));
+        sink.addf(1, bin, __longlong_as_double(vy));
+        sink.addf(2, bin, __longlong_as_double(vz));
+        ++c.zhs;
+      }
+    }
+  }
+}
 
 __device__ __forceinline__ uint32_t find_event(EventPlan const* events, uint32_t n, uint64_t item) {
   uint32_t lo = 0, hi = n;  // last event with first_item <= item
@@ -663,8 +784,16 @@ __global__ void __launch_bounds__(kWindowThreadsMax, 1)
       for (uint64_t i = begin + threadIdx.x; i < end; i += blockDim.x)
         coreas_pair<kFixed, Amp>(load_track(ev.tracks, ev.stride, i), ev.propagation, o, sink, c);
     } else {
-      for (uint64_t i = begin + threadIdx.x; i < end; i += blockDim.x)
-        zhs_pair<kFixed, Amp>(load_track(ev.tracks, ev.stride, i), ev.propagation, o, sink, c);
+      // uniform trip count: every warp reaches deposit_runs converged
+      for (uint64_t base = begin; base < end; base += blockDim.x) {
+        uint64_t const i = base + threadIdx.x;
+        PendingRange run;
+        run.count = 0;
+        if (i < end)
+          zhs_pair<kFixed, true, Amp>(load_track(ev.tracks, ev.stride, i), ev.propagation, o,
+                                      sink, c, &run);
+        deposit_runs<kFixed>(sink, run, c);
+      }
     }
     __syncthreads();
 
