@@ -193,7 +193,7 @@ class Accumulator {
     precision_ = config.precision == C8R_PRECISION_MIXED ? Precision::kMixed : Precision::kFP64;
     kernel_ = config.kernel;
     host_batch_ = tuning.batch_size ? static_cast<std::size_t>(tuning.batch_size) : kDefaultHostBatch;
-    threads_ = tuning.team_size ? static_cast<int>(tuning.team_size) : 384;
+    threads_ = tuning.team_size ? static_cast<int>(tuning.team_size) : 512;
     upload_static();
     allocate_traces();
     counters_.allocate(1);
@@ -697,27 +697,33 @@ class Accumulator {
     stats_.direct_projection_records += count;
   }
 
+  // One persistent launch per algorithm (CoREAS items, then ZHS items): each
+  // kernel instance carries one algorithm's code only.
   void project_windowed(std::size_t count) {
-    WorkPlan plan{};
-    plan.events[0] = make_event(count);
-    plan.events[0].first_item = 0;
-    uint32_t const per_chunk = plan.events[0].observer_count[0] + plan.events[0].observer_count[1];
-    plan.event_count = 1;
-    plan.window = plan.events[0].window;
-    plan.total_items = static_cast<uint64_t>(plan.events[0].chunks) * per_chunk;
-    plan.next_item = next_item_.ptr;
-    int per_sm = windowed_ctas_per_sm(static_cast<int>(plan.window), threads_, fixed_, precision_);
+    EventPlan const ev = make_event(count);
+    int per_sm = windowed_ctas_per_sm(static_cast<int>(ev.window), threads_, fixed_, precision_);
     if (per_sm <= 0) throw cuda_error("windowed radio kernel does not fit on this device");
-    uint64_t ctas = static_cast<uint64_t>(per_sm) * sms_;
-    if (ctas > plan.total_items) ctas = plan.total_items;
-    check(cudaMemsetAsync(next_item_.ptr, 0, sizeof(unsigned), stream_), "memset");
-    check(launch_windowed(plan, fixed_, precision_, static_cast<int>(ctas), threads_, stream_),
-          "windowed launch");
-    uint64_t const pairs_c = count * plan.events[0].observer_count[0];
-    uint64_t const pairs_z = count * plan.events[0].observer_count[1];
+    for (int algorithm = 0; algorithm < 2; ++algorithm) {
+      if (ev.observer_count[algorithm] == 0) continue;
+      WorkPlan plan{};
+      plan.events[0] = ev;
+      plan.events[0].first_item = 0;
+      plan.algorithm = algorithm;
+      plan.event_count = 1;
+      plan.window = ev.window;
+      plan.total_items = static_cast<uint64_t>(ev.chunks) * ev.observer_count[algorithm];
+      plan.next_item = next_item_.ptr;
+      uint64_t ctas = static_cast<uint64_t>(per_sm) * sms_;
+      if (ctas > plan.total_items) ctas = plan.total_items;
+      check(cudaMemsetAsync(next_item_.ptr, 0, sizeof(unsigned), stream_), "memset");
+      check(launch_windowed(plan, fixed_, precision_, static_cast<int>(ctas), threads_, stream_),
+            "windowed launch");
+      stats_.projection_tiles += plan.total_items;
+    }
+    uint64_t const pairs_c = count * ev.observer_count[0];
+    uint64_t const pairs_z = count * ev.observer_count[1];
     stats_.track_observer_pairs += pairs_c + pairs_z;
     if (fuse_) stats_.fused_track_observer_pairs += pairs_c;
-    stats_.projection_tiles += plan.total_items;
   }
 
   void fetch_counters(DeviceCounters& host) {

@@ -201,6 +201,48 @@ struct PendingRange {
 // Runs shorter than this are deposited by their own lane.
 constexpr uint32_t kCooperativeRun = 6;
 
+// Near-Cherenkov branch of accumulate_co_reas (RadioProjection.inl:352-387):
+// midpoint field over the Doppler-compressed duration.  Kept out of line: it
+// is taken by a minority of pairs, and its third propagation would otherwise
+// grow the hot loop's instruction footprint.  Returns the counts it adds.
+template <bool kFixed, class Amp, class Sink>
+__device__ __noinline__ Counts coreas_near_cone(Track const t, Propagation const& p,
+                                                ObserverCache const& o, Sink sink,
+                                                bool start_before_end) {
+  Counts c;
+  Vec3<Amp> const beta{static_cast<Amp>(t.bx), static_cast<Amp>(t.by), static_cast<Amp>(t.bz)};
+  double const cf = t.constant * o.sample_rate;
+  double const mx = (t.sx + t.ex) * 0.5, my = (t.sy + t.ey) * 0.5, mz = (t.sz + t.ez) * 0.5;
+  double const mt = (t.ts + t.te) * 0.5;
+  Path const pm = propagate<true>(p, o, mx, my, mz);
+  double const mr = mt + pm.time;
+  double const md = doppler(pm.n_src, t.bx, t.by, t.bz, pm.kx, pm.ky, pm.kz);
+  Vec3<Amp> const k{static_cast<Amp>(pm.kx), static_cast<Amp>(pm.ky), static_cast<Amp>(pm.kz)};
+  Vec3<Amp> fstart =
+      scaled(cross(k, cross(k, beta)), amp_div(static_cast<Amp>(cf), static_cast<Amp>(md * pm.dist)));
+  Vec3<Amp> fend = scaled(fstart, static_cast<Amp>(-1.));
+  double dt = t.length / (kSpeedOfLight * t.beta_module) * fabs(md);
+  double sr, er;
+  if (start_before_end) {
+    sr = mr - 0.5 * dt;
+    er = mr + 0.5 * dt;
+  } else {
+    sr = mr + 0.5 * dt;
+    er = mr - 0.5 * dt;
+  }
+  double const res = o.resolution;
+  dt = er - sr;
+  if (fabs(dt) < res) {
+    Amp const s = static_cast<Amp>(fabs(dt / res));
+    fstart = scaled(fstart, s);
+    fend = scaled(fend, s);
+    separate_same_bin(sr, er, res, true);
+  }
+  add_sample<false, kFixed>(o, sink, sr, fstart, c.coreas, c.overflows);
+  add_sample<false, kFixed>(o, sink, er, fend, c.coreas, c.overflows);
+  return c;
+}
+
 // ---------------------------------------------------------------- CoREAS
 // accumulate_co_reas, RadioProjection.inl:339-409.
 template <bool kFixed, class Amp, class Sink>
@@ -216,33 +258,9 @@ __device__ __forceinline__ void coreas_pair(Track const& t, Propagation const& p
   Vec3<Amp> const beta{static_cast<Amp>(t.bx), static_cast<Amp>(t.by), static_cast<Amp>(t.bz)};
 
   if (ps.n_dst > 1. && (fabs(pre) < kCoreasThreshold || fabs(post) < kCoreasThreshold)) {
-    double const mx = (t.sx + t.ex) * 0.5, my = (t.sy + t.ey) * 0.5, mz = (t.sz + t.ez) * 0.5;
-    double const mt = (t.ts + t.te) * 0.5;
-    Path const pm = propagate<true>(p, o, mx, my, mz);
-    double const mr = mt + pm.time;
-    double const md = doppler(pm.n_src, t.bx, t.by, t.bz, pm.kx, pm.ky, pm.kz);
-    Vec3<Amp> const k{static_cast<Amp>(pm.kx), static_cast<Amp>(pm.ky), static_cast<Amp>(pm.kz)};
-    Vec3<Amp> fstart =
-        scaled(cross(k, cross(k, beta)), amp_div(static_cast<Amp>(cf), static_cast<Amp>(md * pm.dist)));
-    Vec3<Amp> fend = scaled(fstart, static_cast<Amp>(-1.));
-    double dt = t.length / (kSpeedOfLight * t.beta_module) * fabs(md);
-    if (sr < er) {
-      sr = mr - 0.5 * dt;
-      er = mr + 0.5 * dt;
-    } else {
-      sr = mr + 0.5 * dt;
-      er = mr - 0.5 * dt;
-    }
-    double const res = o.resolution;
-    dt = er - sr;
-    if (fabs(dt) < res) {
-      Amp const s = static_cast<Amp>(fabs(dt / res));
-      fstart = scaled(fstart, s);
-      fend = scaled(fend, s);
-      separate_same_bin(sr, er, res, true);
-    }
-    add_sample<false, kFixed>(o, sink, sr, fstart, c.coreas, c.overflows);
-    add_sample<false, kFixed>(o, sink, er, fend, c.coreas, c.overflows);
+    Counts const d = coreas_near_cone<kFixed, Amp>(t, p, o, sink, sr < er);
+    c.coreas += d.coreas;
+    c.overflows += d.overflows;
     return;
   }
 
@@ -264,6 +282,31 @@ __device__ __forceinline__ void coreas_pair(Track const& t, Propagation const& p
   }
   add_sample<false, kFixed>(o, sink, sr, fstart, c.coreas, c.overflows);
   add_sample<false, kFixed>(o, sink, er, fend, c.coreas, c.overflows);
+}
+
+// Intermediate ZHS bins binned index by index with the reference's own
+// expression (RadioProjection.inl:465-472).  Samples of index i land in bin
+// nearest((d1 + i/fs - t0) fs), monotone in i and within a hundredth of a bin
+// of x1 + i while all magnitudes stay below 2^40 bins; indices whose bin is
+// surely outside [0, bins) are skipped, which changes no sum and no counter.
+template <bool kFixed, class Amp, class Sink>
+__device__ __noinline__ Counts zhs_indexed_bins(ObserverCache const& o, Sink sink, double d1,
+                                                double x1, int nb, Deposit<Amp> const mid) {
+  Counts c;
+  double const fs = o.sample_rate;
+  int lo = 1, hi = nb;
+  double const span = 1099511627776.0;  // 2^40
+  if (fabs(x1) < span && fabs(o.start_time * fs) < span && fabs(d1 * fs) < span &&
+      static_cast<double>(nb) < span) {
+    double const first = -x1 - 3.;
+    double const last = o.bins_d - x1 + 3.;
+    if (first > 1.) lo = first >= static_cast<double>(nb) ? nb : static_cast<int>(first);
+    if (last < static_cast<double>(nb)) hi = last <= 1. ? 1 : static_cast<int>(last) + 1;
+    if (hi > nb) hi = nb;
+  }
+  for (int index = lo; index < hi; ++index)
+    deposit<true, kFixed>(o, sink, d1 + static_cast<double>(index) / fs, mid, c.zhs, c.overflows);
+  return c;
 }
 
 // ---------------------------------------------------------------- ZHS
@@ -372,22 +415,9 @@ __device__ __forceinline__ void zhs_segment(double p1x, double p1y, double p1z, 
       }
     }
     if (!binned) {
-    // Samples of index i land in bin nearest((d1 + i/fs - t0) fs), monotone in i
-    // and within a hundredth of a bin of x1 + i while all magnitudes stay below
-    // 2^40 bins; indices whose bin is surely outside [0, bins) are skipped,
-    // which changes no sum and no counter.
-    int lo = 1, hi = nb;
-    double const span = 1099511627776.0;  // 2^40
-    if (fabs(x1) < span && fabs(o.start_time * fs) < span && fabs(d1 * fs) < span &&
-        static_cast<double>(nb) < span) {
-      double const first = -x1 - 3.;
-      double const last = o.bins_d - x1 + 3.;
-      if (first > 1.) lo = first >= static_cast<double>(nb) ? nb : static_cast<int>(first);
-      if (last < static_cast<double>(nb)) hi = last <= 1. ? 1 : static_cast<int>(last) + 1;
-      if (hi > nb) hi = nb;
-    }
-    for (int index = lo; index < hi; ++index)
-      deposit<true, kFixed>(o, sink, d1 + static_cast<double>(index) / fs, mid, c.zhs, c.overflows);
+      Counts const d = zhs_indexed_bins<kFixed, Amp>(o, sink, d1, x1, nb, mid);
+      c.zhs += d.zhs;
+      c.overflows += d.overflows;
     }
   }
   frac = fabs(x2 + 0.5 - eb);
@@ -414,29 +444,26 @@ __device__ __forceinline__ void zhs_pair(Track const& t, Propagation const& p,
   }
   c.subtracks += static_cast<unsigned long long>(static_cast<long long>(subtracks));
   int const refinement = static_cast<int>(p.refinement);
-  if (subtracks == 1 && refinement == 1) {
-    // divisor is exactly 1: point2 = start + (end - start), time2 likewise
-    zhs_segment<kFixed, kRuns, Amp>(t.sx, t.sy, t.sz, t.sx + (t.ex - t.sx),
-                                    t.sy + (t.ey - t.sy), t.sz + (t.ez - t.sz), t.ts,
-                                    t.ts + (t.te - t.ts), t, p, o, sink, c, false, pending);
-    return;
-  }
+  // One segment when undivided: the loop below then evaluates
+  // point2 = start + (end - start) / 1 / 1, exactly the reference's values.
+  bool const subdivided = subtracks > 1 || refinement > 1;
   double const rd = static_cast<double>(refinement);
   double const rx = (t.ex - t.sx) / divisor / rd;
   double const ry = (t.ey - t.sy) / divisor / rd;
   double const rz = (t.ez - t.sz) / divisor / rd;
   double const rt = (t.te - t.ts) / divisor / rd;
   double p1x = t.sx, p1y = t.sy, p1z = t.sz, t1 = t.ts;
-  for (int index = 0; index < subtracks; ++index) {
-    for (int r = 0; r < refinement; ++r) {
-      double const p2x = p1x + rx, p2y = p1y + ry, p2z = p1z + rz, t2 = t1 + rt;
-      zhs_segment<kFixed, kRuns, Amp>(p1x, p1y, p1z, p2x, p2y, p2z, t1, t2, t, p, o, sink, c,
-                                      true, pending);
-      p1x = p2x;
-      p1y = p2y;
-      p1z = p2z;
-      t1 = t2;
-    }
+  // subtrack-major, refinement-minor order of the reference's nested loops
+  long long const segments = static_cast<long long>(subtracks) * refinement;
+#pragma unroll 1
+  for (long long index = 0; index < segments; ++index) {
+    double const p2x = p1x + rx, p2y = p1y + ry, p2z = p1z + rz, t2 = t1 + rt;
+    zhs_segment<kFixed, kRuns, Amp>(p1x, p1y, p1z, p2x, p2y, p2z, t1, t2, t, p, o, sink, c,
+                                    subdivided, pending);
+    p1x = p2x;
+    p1y = p2y;
+    p1z = p2z;
+    t1 = t2;
   }
   if (refinement > 1)
     c.subtracks += static_cast<unsigned long long>(
@@ -659,7 +686,7 @@ __global__ void __launch_bounds__(256) ingest_kernel(
 
 // ---------------------------------------------------------------- direct
 template <bool kFixed, class Amp, bool kCoreas, bool kZhs>
-__global__ void __launch_bounds__(256) direct_kernel(EventPlan ev) {
+__global__ void __launch_bounds__(256) direct_kernel(const __grid_constant__ EventPlan ev) {
   uint64_t const tracks = *ev.valid_tracks;
   uint32_t const observers =
       ev.observer_count[0] > ev.observer_count[1] ? ev.observer_count[0] : ev.observer_count[1];
@@ -741,11 +768,12 @@ __device__ __forceinline__ uint32_t find_event(EventPlan const* events, uint32_t
   return lo;
 }
 
-template <bool kFixed, class Amp>
+template <bool kFixed, class Amp, int kAlgorithm>
 __global__ void __launch_bounds__(kWindowThreadsMax, 1)
     windowed_kernel(const __grid_constant__ WorkPlan plan) {
   extern __shared__ __align__(16) unsigned long long window[];
   __shared__ unsigned long long item_shared;
+  __shared__ ObserverCache observer;
   Counts c;
   for (;;) {
     __syncthreads();
@@ -754,18 +782,19 @@ __global__ void __launch_bounds__(kWindowThreadsMax, 1)
     uint64_t const item = item_shared;
     if (item >= plan.total_items) break;
     EventPlan const& ev = plan.events[find_event(plan.events, plan.event_count, item)];
+    constexpr int algorithm = kAlgorithm;
     uint64_t const local = item - ev.first_item;
-    uint32_t const per_chunk = ev.observer_count[0] + ev.observer_count[1];
+    uint32_t const per_chunk = ev.observer_count[algorithm];
     uint64_t const chunk = local / per_chunk;
-    uint32_t const r = static_cast<uint32_t>(local - chunk * per_chunk);
-    int const algorithm = r < ev.observer_count[0] ? 0 : 1;
-    uint32_t const oi = algorithm ? r - ev.observer_count[0] : r;
+    uint32_t const oi = static_cast<uint32_t>(local - chunk * per_chunk);
     uint64_t const track_count = *ev.valid_tracks;
     uint64_t const begin = chunk * ev.chunk_size;
     if (begin >= track_count) continue;
     uint64_t const end = begin + ev.chunk_size < track_count ? begin + ev.chunk_size : track_count;
-    ObserverCache const o = ev.observers[algorithm][oi];
-    uint32_t const width = static_cast<uint32_t>(o.bins < ev.window ? o.bins : ev.window);
+    if (threadIdx.x == 0) observer = ev.observers[algorithm][oi];
+    ObserverCache const& o = observer;
+    uint64_t const bins = ev.observers[algorithm][oi].bins;
+    uint32_t const width = static_cast<uint32_t>(bins < ev.window ? bins : ev.window);
 
     // zero the window (3 rows of width bins)
     for (uint32_t j = threadIdx.x; j < 3 * width; j += blockDim.x) window[j] = 0ull;
@@ -780,7 +809,7 @@ __global__ void __launch_bounds__(kWindowThreadsMax, 1)
       sink.row[row] = kFixed ? ev.fixed[algorithm] + row * total + o.offset : nullptr;
       sink.frow[row] = kFixed ? nullptr : ev.floating[algorithm] + row * total + o.offset;
     }
-    if (algorithm == 0) {
+    if (kAlgorithm == 0) {
       for (uint64_t i = begin + threadIdx.x; i < end; i += blockDim.x)
         coreas_pair<kFixed, Amp>(load_track(ev.tracks, ev.stride, i), ev.propagation, o, sink, c);
     } else {
@@ -852,27 +881,39 @@ cudaError_t direct_dispatch(EventPlan const& ev, uint64_t bound, bool coreas, bo
   return cudaGetLastError();
 }
 
-template <bool kFixed, class Amp>
-cudaError_t windowed_dispatch(WorkPlan const& plan, int ctas, int threads, cudaStream_t stream) {
+template <bool kFixed, class Amp, int kAlgorithm>
+cudaError_t windowed_dispatch_algorithm(WorkPlan const& plan, int ctas, int threads,
+                                        cudaStream_t stream) {
   size_t const bytes = static_cast<size_t>(plan.window) * 3 * sizeof(unsigned long long);
-  cudaError_t err = cudaFuncSetAttribute(windowed_kernel<kFixed, Amp>,
+  cudaError_t err = cudaFuncSetAttribute(windowed_kernel<kFixed, Amp, kAlgorithm>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(bytes));
   if (err != cudaSuccess) return err;
-  windowed_kernel<kFixed, Amp><<<ctas, threads, bytes, stream>>>(plan);
+  windowed_kernel<kFixed, Amp, kAlgorithm><<<ctas, threads, bytes, stream>>>(plan);
   return cudaGetLastError();
+}
+
+template <bool kFixed, class Amp>
+cudaError_t windowed_dispatch(WorkPlan const& plan, int ctas, int threads, cudaStream_t stream) {
+  return plan.algorithm == 0
+             ? windowed_dispatch_algorithm<kFixed, Amp, 0>(plan, ctas, threads, stream)
+             : windowed_dispatch_algorithm<kFixed, Amp, 1>(plan, ctas, threads, stream);
 }
 
 template <bool kFixed, class Amp>
 int ctas_per_sm(int window, int threads) {
   size_t const bytes = static_cast<size_t>(window) * 3 * sizeof(unsigned long long);
-  cudaFuncSetAttribute(windowed_kernel<kFixed, Amp>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       static_cast<int>(bytes));
-  int blocks = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, windowed_kernel<kFixed, Amp>, threads,
-                                                    bytes) != cudaSuccess)
-    return 0;
-  return blocks;
+  int worst = 1 << 30;
+  auto probe = [&](auto kernel) {
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
+    int blocks = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, threads, bytes) != cudaSuccess)
+      blocks = 0;
+    worst = blocks < worst ? blocks : worst;
+  };
+  probe(windowed_kernel<kFixed, Amp, 0>);
+  probe(windowed_kernel<kFixed, Amp, 1>);
+  return worst;
 }
 
 }  // namespace

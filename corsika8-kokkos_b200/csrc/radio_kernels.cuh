@@ -51,7 +51,7 @@ struct EventPlan {
   uint64_t total_bins[2];
   Propagation propagation;
   DeviceCounters* counters;
-  uint64_t first_item;           // work-list offset of this event
+  uint64_t first_item;           // work-list offset of this event (in its algorithm's list)
   uint32_t chunk_size;           // tracks per work item
   uint32_t chunks;
   uint32_t window;               // shared-memory bins per item (<= kernel window)
@@ -65,6 +65,7 @@ constexpr int kMaxEventsPerLaunch = 64;
 constexpr int kWindowThreads = 512;  // upper bound of the windowed block size
 struct WorkPlan {
   EventPlan events[kMaxEventsPerLaunch];
+  int32_t algorithm;        // 0: CoREAS items, 1: ZHS items
   uint32_t event_count;
   uint32_t window;          // shared-memory bins per CTA (max over events)
   uint64_t total_items;
