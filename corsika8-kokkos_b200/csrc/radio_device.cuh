@@ -121,15 +121,25 @@ __device__ __forceinline__ double doppler(double index, double bx, double by, do
 
 // propagate, RadioProjection.inl:170-238.  kTime = false skips the refractive
 // index and travel time (the Fraunhofer midpoint uses only k and distance).
-template <bool kTime>
+// kApproxDirection = true returns k = d * RN(1/|d|): each component within
+// 3.01 u |k| of the reference's RN(d/|d|) (u = 2^-53); distance, refractive
+// indices and travel time are exact in both forms.
+template <bool kTime, bool kApproxDirection = false>
 __device__ __forceinline__ Path propagate(Propagation const& p, ObserverCache const& o,
                                           double sx, double sy, double sz) {
   Path r;
   double const dx = o.px - sx, dy = o.py - sy, dz = o.pz - sz;
   double const dist = sqrt(dx * dx + dy * dy + dz * dz);
-  r.kx = dx / dist;
-  r.ky = dy / dist;
-  r.kz = dz / dist;
+  if (kApproxDirection) {
+    double const inverse = 1. / dist;
+    r.kx = dx * inverse;
+    r.ky = dy * inverse;
+    r.kz = dz * inverse;
+  } else {
+    r.kx = dx / dist;
+    r.ky = dy / dist;
+    r.kz = dz / dist;
+  }
   r.dist = dist;
   if (!kTime) return r;
   if (p.homogeneous > 0.) {

@@ -244,7 +244,8 @@ __device__ __noinline__ Counts coreas_near_cone(Track const t, Propagation const
 }
 
 // ---------------------------------------------------------------- CoREAS
-// accumulate_co_reas, RadioProjection.inl:339-409.
+// accumulate_co_reas, RadioProjection.inl:339-409, every decision and (FP64
+// path) every amplitude evaluated exactly as the reference.
 template <bool kFixed, class Amp, class Sink>
 __device__ __forceinline__ void coreas_pair(Track const& t, Propagation const& p,
                                             ObserverCache const& o, Sink& sink, Counts& c) {
@@ -270,6 +271,75 @@ __device__ __forceinline__ void coreas_pair(Track const& t, Propagation const& p
       scaled(cross(ks, cross(ks, beta)), amp_div(static_cast<Amp>(cf), static_cast<Amp>(pre * ps.dist)));
   Vec3<Amp> fend =
       scaled(cross(ke, cross(ke, beta)), amp_div(static_cast<Amp>(-cf), static_cast<Amp>(post * pe.dist)));
+  if (pre < 1.e-9 || post < 1.e-9) {
+    double const res = o.resolution;
+    double const dt = er - sr;
+    if (fabs(dt) < res) {
+      Amp const s = static_cast<Amp>(fabs(dt / res));
+      fstart = scaled(fstart, s);
+      fend = scaled(fend, s);
+      separate_same_bin(sr, er, res, false);
+    }
+  }
+  add_sample<false, kFixed>(o, sink, sr, fstart, c.coreas, c.overflows);
+  add_sample<false, kFixed>(o, sink, er, fend, c.coreas, c.overflows);
+}
+
+// The exact pair out of line: the filtered path's fallback.
+template <bool kFixed, class Amp, class Sink>
+__device__ __noinline__ Counts coreas_pair_exact(Track const t, Propagation const& p,
+                                                 ObserverCache const& o, Sink sink) {
+  Counts c;
+  coreas_pair<kFixed, Amp>(t, p, o, sink, c);
+  return c;
+}
+
+// Mixed-precision CoREAS pair.  Travel times, refractive indices and
+// distances are exact; emission directions are d * RN(1/|d|) (propagate's
+// kApproxDirection), so each Doppler factor 1 - n beta.k lies within
+// 14 u n |beta|_1 + 2 u of the reference's (u = 2^-53; bound below used with
+// a 4.5x margin).  The pair's branches (near-Cherenkov |doppler| < 1e-3, the
+// sign test doppler < 1e-9) are taken only when that bound cannot move them;
+// any pair closer than the bound to a threshold, or with |doppler| < 1e-6,
+// is evaluated exactly.  Sample times are exact, so bins are the reference's.
+template <bool kFixed, class Amp, class Sink>
+__device__ __forceinline__ void coreas_pair_filtered(Track const& t, Propagation const& p,
+                                                     ObserverCache const& o, Sink& sink,
+                                                     Counts& c) {
+  Path const ps = propagate<true, true>(p, o, t.sx, t.sy, t.sz);
+  Path const pe = propagate<true, true>(p, o, t.ex, t.ey, t.ez);
+  double const pre = 1. - ps.n_src * (t.bx * ps.kx + t.by * ps.ky + t.bz * ps.kz);
+  double const post = 1. - pe.n_src * (t.bx * pe.kx + t.by * pe.ky + t.bz * pe.kz);
+  double const beta1 = fabs(t.bx) + fabs(t.by) + fabs(t.bz) + 1.;
+  double const err_pre = ps.n_src * beta1 * 0x1p-47 + 0x1p-50;
+  double const err_post = pe.n_src * beta1 * 0x1p-47 + 0x1p-50;
+  bool const ambiguous =
+      fabs(pre) < 1.e-6 || fabs(post) < 1.e-6 ||
+      (ps.n_dst > 1. && (fabs(fabs(pre) - kCoreasThreshold) <= err_pre ||
+                         fabs(fabs(post) - kCoreasThreshold) <= err_post));
+  if (ambiguous) {
+    Counts const d = coreas_pair_exact<kFixed, Amp>(t, p, o, sink);
+    c.coreas += d.coreas;
+    c.overflows += d.overflows;
+    return;
+  }
+  double sr = t.ts + ps.time;
+  double er = t.te + pe.time;
+  if (ps.n_dst > 1. && (fabs(pre) < kCoreasThreshold || fabs(post) < kCoreasThreshold)) {
+    Counts const d = coreas_near_cone<kFixed, Amp>(t, p, o, sink, sr < er);
+    c.coreas += d.coreas;
+    c.overflows += d.overflows;
+    return;
+  }
+  Vec3<Amp> const beta{static_cast<Amp>(t.bx), static_cast<Amp>(t.by), static_cast<Amp>(t.bz)};
+  Vec3<Amp> const ks{static_cast<Amp>(ps.kx), static_cast<Amp>(ps.ky), static_cast<Amp>(ps.kz)};
+  Vec3<Amp> const ke{static_cast<Amp>(pe.kx), static_cast<Amp>(pe.ky), static_cast<Amp>(pe.kz)};
+  Amp const cf = static_cast<Amp>(t.constant * o.sample_rate);
+  Vec3<Amp> fstart =
+      scaled(cross(ks, cross(ks, beta)), amp_div(cf, static_cast<Amp>(pre * ps.dist)));
+  Vec3<Amp> fend =
+      scaled(cross(ke, cross(ke, beta)), amp_div(-cf, static_cast<Amp>(post * pe.dist)));
+  // |pre|, |post| >= 1e-6 here, so "< 1e-9" is the sign of the factor
   if (pre < 1.e-9 || post < 1.e-9) {
     double const res = o.resolution;
     double const dt = er - sr;
@@ -310,6 +380,13 @@ __device__ __noinline__ Counts zhs_indexed_bins(ObserverCache const& o, Sink sin
 }
 
 // ---------------------------------------------------------------- ZHS
+template <bool kFixed, class Amp, class Sink>
+__device__ __noinline__ Counts zhs_segment_exact(double p1x, double p1y, double p1z, double p2x,
+                                                 double p2y, double p2z, double t1, double t2,
+                                                 Track const t, Propagation const& p,
+                                                 ObserverCache const& o, Sink sink,
+                                                 bool subdivided);
+
 // accumulate_zhs_segment, RadioProjection.inl:412-480.
 //
 // kRuns = true (windowed kernel): the intermediate bins of a segment are the
@@ -318,19 +395,35 @@ __device__ __noinline__ Counts zhs_indexed_bins(ObserverCache const& o, Sink sin
 // without the per-index division, and long runs are handed to the warp via
 // `pending`.  Otherwise, and always for kRuns = false (the reference-shaped
 // direct kernel), each index is binned by the reference's own expression.
-template <bool kFixed, bool kRuns, class Amp, class Sink>
+//
+// kFilter = true (mixed precision): the emission direction is d * RN(1/|d|),
+// so n beta.k lies within e_nbk of the reference's value and each detection
+// time within e_d; every decision the segment takes (which detection time is
+// first, the nearest bin and floor(x + 0.5) of both, |1 - n beta.k| > 1e-15,
+// the consecutive-run test) is taken only when those bounds cannot change it,
+// else the segment is evaluated exactly.  Bins and counts are the reference's.
+template <bool kFixed, bool kRuns, bool kFilter, class Amp, class Sink>
 __device__ __forceinline__ void zhs_segment(double p1x, double p1y, double p1z, double p2x,
                                             double p2y, double p2z, double t1, double t2,
                                             Track const& t, Propagation const& p,
                                             ObserverCache const& o, Sink& sink, Counts& c,
                                             bool subdivided, PendingRange* pending) {
   double const mx = (p1x + p2x) * 0.5, my = (p1y + p2y) * 0.5, mz = (p1z + p2z) * 0.5;
-  Path const path = propagate<true>(p, o, mx, my, mz);
+  Path const path = propagate<true, kFilter>(p, o, mx, my, mz);
   double const bk = t.bx * path.kx + t.by * path.ky + t.bz * path.kz;
   double const nbk = path.n_src * bk;
   double const mt = (t1 + t2) * 0.5;
   double d1 = t1 + path.time - nbk * (t1 - mt);
   double d2 = t2 + path.time - nbk * (t2 - mt);
+  double e_d = 0.;
+  if (kFilter) {
+    // |nbk - reference| <= 11.1 u n |beta|_1; each d within that times
+    // |t - mt| plus two ulps of its terms (bounds used with margins >= 4x)
+    double const beta1 = fabs(t.bx) + fabs(t.by) + fabs(t.bz) + 1.;
+    double const e_nbk = path.n_src * beta1 * 0x1p-47 + 0x1p-50;
+    double const h = fabs(t1 - mt) + fabs(t2 - mt);
+    e_d = e_nbk * h + 0x1p-50 * (fabs(t1 + path.time) + fabs(t2 + path.time) + fabs(nbk) * h);
+  }
   double sign = 1.;
   if (d1 > d2) {
     double const swap = d1;
@@ -343,104 +436,149 @@ __device__ __forceinline__ void zhs_segment(double p1x, double p1y, double p1z, 
   double const x2 = (d2 - o.start_time) * fs;
   double const sb = floor(x1 + 0.5);
   double const eb = floor(x2 + 0.5);
+  double const den = 1. - nbk;
+  int const nb = x86_int(eb - sb);
+  // consecutive-run test for the intermediate bins.  Index i is binned at
+  // y_i = RN(RN(RN(d1 + RN(i/fs)) - t0) fs); with u = 2^-53,
+  // |y_i - (x1 + i)| <= 6 u M (1 + u)^4 < 2^-50 M for M = |x1| + i + |d1 fs|
+  // + |t0 fs| + 2.  The nearest bin changes only at half-integers, which sit
+  // at integer offsets from each other, so if x1 is farther than that bound
+  // (plus, filtered, x1's own error) from a half-integer, nearest(y_i) =
+  // nearest(x1) + i for every i < nb.
+  double const f1 = fabs(x1 - floor(x1) - 0.5);
+  double const mag = fabs(x1) + static_cast<double>(nb) + fabs(d1 * fs) + fabs(o.start_time * fs) + 2.;
+  bool run_ok = mag < 0x1p50 && f1 > mag * 0x1p-48;
+  if (kFilter) {
+    double const e_x = (e_d + 0x1p-50 * (fabs(d1) + fabs(d2) + 2. * fabs(o.start_time))) * fs +
+                       0x1p-50 * (fabs(x1) + fabs(x2));
+    double const f2 = fabs(x2 - floor(x2) - 0.5);
+    run_ok = run_ok && f1 > mag * 0x1p-48 + e_x;
+    bool const ambiguous = fabs(d1 - d2) <= 2. * e_d || fabs(den) < 1.e-6 ||
+                           f1 <= e_x + 0x1p-50 * (fabs(x1) + 1.) ||
+                           f2 <= e_x + 0x1p-50 * (fabs(x2) + 1.) || (nb > 1 && !run_ok);
+    if (ambiguous) {
+      Counts const d = zhs_segment_exact<kFixed, Amp>(p1x, p1y, p1z, p2x, p2y, p2z, t1, t2, t, p,
+                                                      o, sink, subdivided);
+      c.zhs += d.zhs;
+      c.overflows += d.overflows;
+      return;
+    }
+  }
   Vec3<Amp> const k{static_cast<Amp>(path.kx), static_cast<Amp>(path.ky), static_cast<Amp>(path.kz)};
   Vec3<Amp> const beta{static_cast<Amp>(t.bx), static_cast<Amp>(t.by), static_cast<Amp>(t.bz)};
   Vec3<Amp> const perp = cross(k, cross(beta, k));
-  double const den = 1. - nbk;
   double const sc = sign * t.constant;
   double const dd = den * path.dist;
 
-  if (sb == eb) {
-    Vec3<Amp> pot;
-    if (fabs(den) > 1.e-15) {
-      double const frac = fabs(d2 * fs - d1 * fs);
-      pot = scaled(perp, amp_div(static_cast<Amp>(sc * frac), static_cast<Amp>(dd)));
-    } else {
-      double const frac = (t2 - t1) * fs;
-      pot = scaled(perp, amp_div(static_cast<Amp>(sc * frac), static_cast<Amp>(path.dist)));
-    }
-    add_sample<true, kFixed>(o, sink, d2, pot, c.zhs, c.overflows);
-    return;
-  }
-  int const nb = x86_int(eb - sb);
-  double frac = fabs(sb + 0.5 - x1);
+  // The last sample (detection_time2) and, when both times share a bin, the
+  // only one (:441-455); fraction and denominator selected, not branched.
+  bool const single = sb == eb;
+  bool const tiny = !(fabs(den) > 1.e-15);
+  double const frac_last = single ? (tiny ? (t2 - t1) * fs : fabs(d2 * fs - d1 * fs))
+                                  : fabs(x2 + 0.5 - eb);
+  double const den_last = single && tiny ? path.dist : dd;
+  add_sample<true, kFixed>(o, sink, d2,
+                           scaled(perp, amp_div(static_cast<Amp>(sc * frac_last),
+                                                static_cast<Amp>(den_last))),
+                           c.zhs, c.overflows);
+  if (single) return;
+  double const frac_first = fabs(sb + 0.5 - x1);
   add_sample<true, kFixed>(o, sink, d1,
-                           scaled(perp, amp_div(static_cast<Amp>(sc * frac), static_cast<Amp>(dd))),
+                           scaled(perp, amp_div(static_cast<Amp>(sc * frac_first), static_cast<Amp>(dd))),
                            c.zhs, c.overflows);
   if (nb > 1) {
     double const mc = (subdivided ? 1. : sign) * t.constant;
     Deposit<Amp> const mid =
         make_deposit<kFixed>(o, scaled(perp, amp_div(static_cast<Amp>(mc), static_cast<Amp>(dd))));
-    bool binned = false;
-    if (kRuns) {
-      // Index i is binned at y_i = RN(RN(RN(d1 + RN(i/fs)) - t0) fs).  With
-      // u = 2^-53, |y_i - (x1 + i)| <= 6 u M (1 + u)^4 < 2^-50 M for
-      // M = |x1| + i + |d1 fs| + |t0 fs| + 2 (each of the four roundings, and
-      // the two of x1, contribute at most u times a term bounded by M).  The
-      // nearest bin changes only at half-integers, which sit at integer
-      // offsets from each other, so if x1 is farther than that bound from a
-      // half-integer, nearest(y_i) = nearest(x1) + i for every i < nb.
-      double const mag = fabs(x1) + static_cast<double>(nb) + fabs(d1 * fs) +
-                         fabs(o.start_time * fs) + 2.;
-      double const fl = floor(x1);
-      double const f = x1 - fl;
-      if (mag < 0x1p50 && fabs(f - 0.5) > mag * 0x1p-48) {
-        long long const b1 = static_cast<long long>(fl) + (f >= 0.5 ? 1 : 0);
-        long long lo = 1, hi = nb;
-        if (-b1 > lo) lo = -b1;
-        long long const top = static_cast<long long>(o.bins) - b1;
-        if (top < hi) hi = top;
-        if (hi > lo) {
-          uint64_t const first = static_cast<uint64_t>(b1 + lo);
-          uint32_t const count = static_cast<uint32_t>(hi - lo);
-          bool const all_ok = !kFixed || (mid.okx && mid.oky && mid.okz);
-          if (pending && all_ok && count >= kCooperativeRun && pending->count == 0) {
-            pending->bin = first;
-            pending->count = count;
-            if (kFixed) {
-              pending->v[0] = mid.ix;
-              pending->v[1] = mid.iy;
-              pending->v[2] = mid.iz;
-            } else {
-              pending->v[0] = __double_as_longlong(static_cast<double>(mid.value.x));
-              pending->v[1] = __double_as_longlong(static_cast<double>(mid.value.y));
-              pending->v[2] = __double_as_longlong(static_cast<double>(mid.value.z));
-            }
+    if (kRuns && run_ok) {
+      long long const b1 = static_cast<long long>(floor(x1)) + (x1 - floor(x1) >= 0.5 ? 1 : 0);
+      long long lo = 1, hi = nb;
+      if (-b1 > lo) lo = -b1;
+      long long const top = static_cast<long long>(o.bins) - b1;
+      if (top < hi) hi = top;
+      if (hi > lo) {
+        uint64_t const first = static_cast<uint64_t>(b1 + lo);
+        uint32_t const count = static_cast<uint32_t>(hi - lo);
+        bool const all_ok = !kFixed || (mid.okx && mid.oky && mid.okz);
+        if (pending && all_ok && count >= kCooperativeRun && pending->count == 0) {
+          pending->bin = first;
+          pending->count = count;
+          if (kFixed) {
+            pending->v[0] = mid.ix;
+            pending->v[1] = mid.iy;
+            pending->v[2] = mid.iz;
           } else {
-            for (uint32_t k = 0; k < count; ++k)
-              deposit_bin<kFixed>(sink, first + k, mid, c.zhs, c.overflows);
+            pending->v[0] = __double_as_longlong(static_cast<double>(mid.value.x));
+            pending->v[1] = __double_as_longlong(static_cast<double>(mid.value.y));
+            pending->v[2] = __double_as_longlong(static_cast<double>(mid.value.z));
           }
+        } else {
+          for (uint32_t j = 0; j < count; ++j)
+            deposit_bin<kFixed>(sink, first + j, mid, c.zhs, c.overflows);
         }
-        binned = true;
       }
-    }
-    if (!binned) {
+    } else {
       Counts const d = zhs_indexed_bins<kFixed, Amp>(o, sink, d1, x1, nb, mid);
       c.zhs += d.zhs;
       c.overflows += d.overflows;
     }
   }
-  frac = fabs(x2 + 0.5 - eb);
-  add_sample<true, kFixed>(o, sink, d2,
-                           scaled(perp, amp_div(static_cast<Amp>(sc * frac), static_cast<Amp>(dd))),
-                           c.zhs, c.overflows);
+}
+
+// The exact segment out of line: the filtered path's fallback.
+template <bool kFixed, class Amp, class Sink>
+__device__ __noinline__ Counts zhs_segment_exact(double p1x, double p1y, double p1z, double p2x,
+                                                 double p2y, double p2z, double t1, double t2,
+                                                 Track const t, Propagation const& p,
+                                                 ObserverCache const& o, Sink sink,
+                                                 bool subdivided) {
+  Counts c;
+  zhs_segment<kFixed, true, false, Amp>(p1x, p1y, p1z, p2x, p2y, p2z, t1, t2, t, p, o, sink, c,
+                                        subdivided, nullptr);
+  return c;
 }
 
 // accumulate_zhs, RadioProjection.inl:483-529.
-template <bool kFixed, bool kRuns, class Amp, class Sink>
+//
+// kFilter: the Fraunhofer number F is first estimated in FP32 as
+// sin^2(theta) K with sin^2 = |beta x d|^2 / (|beta|^2 |d|^2) and
+// K = 2 pi L^2 / (|d| lambda); its distance from the reference's FP64 F is at
+// most 1.7e-6 sqrt(K F) + 1e-6 F + 1e-12 K (cross-product cancellation and
+// the FP32 roundings; used with a 4x margin).  When the estimate lies surely
+// below 1 the track is one undivided segment, exactly as the reference
+// decides; otherwise F is evaluated exactly.
+template <bool kFixed, bool kRuns, bool kFilter, class Amp, class Sink>
 __device__ __forceinline__ void zhs_pair(Track const& t, Propagation const& p,
                                          ObserverCache const& o, Sink& sink, Counts& c,
                                          PendingRange* pending) {
   double const mx = (t.sx + t.ex) * 0.5, my = (t.sy + t.ey) * 0.5, mz = (t.sz + t.ez) * 0.5;
-  Path const pm = propagate<false>(p, o, mx, my, mz);
-  double const uk = (t.bx * pm.kx + t.by * pm.ky + t.bz * pm.kz) / t.beta_module;
-  double const s2 = 1. - uk * uk;
-  double const fraunhofer = s2 * t.length * t.length / pm.dist / o.wavelength * 2. * kPi;
   double divisor = 1.;
   int subtracks = 1;
-  if (fraunhofer > 1.) {
-    divisor = sqrt(fraunhofer) + 1.;
-    subtracks = x86_int(ceil(divisor));
+  bool exact_fraunhofer = true;
+  if (kFilter) {
+    float const dx = static_cast<float>(o.px - mx), dy = static_cast<float>(o.py - my),
+                dz = static_cast<float>(o.pz - mz);
+    float const bx = static_cast<float>(t.bx), by = static_cast<float>(t.by),
+                bz = static_cast<float>(t.bz);
+    float const cx = by * dz - bz * dy, cy = bz * dx - bx * dz, cz = bx * dy - by * dx;
+    float const d2 = dx * dx + dy * dy + dz * dz;
+    float const b2 = bx * bx + by * by + bz * bz;
+    float const length = static_cast<float>(t.length);
+    float const s2 = (cx * cx + cy * cy + cz * cz) / (b2 * d2);
+    float const k = 6.2831853f * length * length / (sqrtf(d2) * static_cast<float>(o.wavelength));
+    float const f = s2 * k;
+    float const margin = 4.e-6f * sqrtf(k * (f + 1.f)) + 4.e-5f * (f + 1.f) + 4.e-12f * k;
+    exact_fraunhofer = !(f + margin < 1.f);
+  }
+  if (exact_fraunhofer) {
+    Path const pm = propagate<false>(p, o, mx, my, mz);
+    double const uk = (t.bx * pm.kx + t.by * pm.ky + t.bz * pm.kz) / t.beta_module;
+    double const s2 = 1. - uk * uk;
+    double const fraunhofer = s2 * t.length * t.length / pm.dist / o.wavelength * 2. * kPi;
+    if (fraunhofer > 1.) {
+      divisor = sqrt(fraunhofer) + 1.;
+      subtracks = x86_int(ceil(divisor));
+    }
   }
   c.subtracks += static_cast<unsigned long long>(static_cast<long long>(subtracks));
   int const refinement = static_cast<int>(p.refinement);
@@ -458,8 +596,8 @@ __device__ __forceinline__ void zhs_pair(Track const& t, Propagation const& p,
 #pragma unroll 1
   for (long long index = 0; index < segments; ++index) {
     double const p2x = p1x + rx, p2y = p1y + ry, p2z = p1z + rz, t2 = t1 + rt;
-    zhs_segment<kFixed, kRuns, Amp>(p1x, p1y, p1z, p2x, p2y, p2z, t1, t2, t, p, o, sink, c,
-                                    subdivided, pending);
+    zhs_segment<kFixed, kRuns, kFilter, Amp>(p1x, p1y, p1z, p2x, p2y, p2z, t1, t2, t, p, o, sink,
+                                             c, subdivided, pending);
     p1x = p2x;
     p1y = p2y;
     p1z = p2z;
@@ -713,7 +851,7 @@ __global__ void __launch_bounds__(256) direct_kernel(const __grid_constant__ Eve
         sink.row[r] = kFixed ? ev.fixed[1] + r * ev.total_bins[1] + o.offset : nullptr;
         sink.frow[r] = kFixed ? nullptr : ev.floating[1] + r * ev.total_bins[1] + o.offset;
       }
-      zhs_pair<kFixed, false, Amp>(t, ev.propagation, o, sink, c, nullptr);
+      zhs_pair<kFixed, false, false, Amp>(t, ev.propagation, o, sink, c, nullptr);
     }
   }
   flush_counts(c, ev.counters);
@@ -809,9 +947,15 @@ __global__ void __launch_bounds__(kWindowThreadsMax, 1)
       sink.row[row] = kFixed ? ev.fixed[algorithm] + row * total + o.offset : nullptr;
       sink.frow[row] = kFixed ? nullptr : ev.floating[algorithm] + row * total + o.offset;
     }
+    constexpr bool kFilter = sizeof(Amp) == sizeof(float);  // mixed precision
     if (kAlgorithm == 0) {
-      for (uint64_t i = begin + threadIdx.x; i < end; i += blockDim.x)
-        coreas_pair<kFixed, Amp>(load_track(ev.tracks, ev.stride, i), ev.propagation, o, sink, c);
+      for (uint64_t i = begin + threadIdx.x; i < end; i += blockDim.x) {
+        if (kFilter)
+          coreas_pair_filtered<kFixed, Amp>(load_track(ev.tracks, ev.stride, i), ev.propagation, o,
+                                            sink, c);
+        else
+          coreas_pair<kFixed, Amp>(load_track(ev.tracks, ev.stride, i), ev.propagation, o, sink, c);
+      }
     } else {
       // uniform trip count: every warp reaches deposit_runs converged
       for (uint64_t base = begin; base < end; base += blockDim.x) {
@@ -819,8 +963,8 @@ __global__ void __launch_bounds__(kWindowThreadsMax, 1)
         PendingRange run;
         run.count = 0;
         if (i < end)
-          zhs_pair<kFixed, true, Amp>(load_track(ev.tracks, ev.stride, i), ev.propagation, o,
-                                      sink, c, &run);
+          zhs_pair<kFixed, true, kFilter, Amp>(load_track(ev.tracks, ev.stride, i),
+                                               ev.propagation, o, sink, c, &run);
         deposit_runs<kFixed>(sink, run, c);
       }
     }
