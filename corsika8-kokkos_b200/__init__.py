@@ -132,6 +132,7 @@ class RadioConfig:
     zhs_observers: np.ndarray = field(default_factory=lambda: np.zeros(0, OBSERVER))
     precision: int = abi.PRECISION_FP64
     kernel: int = abi.KERNEL_AUTO
+    count_samples: bool = False
 
     def to_c(self):
         """Returns (abi.Config, keepalive) with pointers into contiguous copies."""
@@ -158,7 +159,7 @@ class RadioConfig:
             int(self.track_diagnostics), int(self.zhs_subtrack_refinement), prop,
             co.ctypes.data if co.size else None, int(co.size),
             zo.ctypes.data if zo.size else None, int(zo.size),
-            int(self.precision), int(self.kernel),
+            int(self.precision), int(self.kernel), int(self.count_samples), 0,
         )
         return cfg, keep
 

@@ -116,6 +116,8 @@ class Config(C.Structure):
         ("zhs_observer_count", C.c_uint64),
         ("precision", C.c_int32),
         ("kernel", C.c_int32),
+        ("count_samples", C.c_int32),
+        ("reserved_", C.c_int32),
     ]
 
 

@@ -120,6 +120,8 @@ void validate(c8r_config const& config) {
     throw std::invalid_argument("invalid radio precision");
   if (config.kernel < C8R_KERNEL_AUTO || config.kernel > C8R_KERNEL_WINDOWED)
     throw std::invalid_argument("invalid radio kernel selection");
+  if (config.count_samples && !config.deterministic)
+    throw std::invalid_argument("radio sample counting needs fixed-point traces");
   auto check_observers = [&](c8r_observer_snapshot const* observers, uint64_t count) {
     if (count != 0 && observers == nullptr) throw std::invalid_argument("null radio observers");
     for (uint64_t i = 0; i < count; ++i) {
@@ -468,7 +470,7 @@ class Accumulator {
       throw std::length_error("radio track capacity overflow");
     std::size_t const grown = capacity_ == 0 ? count : std::max(count, 2 * capacity_);
     std::size_t const old_bytes = tracks_.bytes();
-    std::size_t const new_bytes = checked_mul(checked_mul(grown, kTrackRows), sizeof(double));
+    std::size_t const new_bytes = checked_mul(checked_mul(grown, kTrackDoubles), sizeof(double));
     retained = current - old_bytes + new_bytes;
     peak = checked_add(current, new_bytes);
   }
@@ -505,6 +507,7 @@ class Accumulator {
     diagnostics_ = config.track_diagnostics != 0;
     limit_ = config.fixed_point_field_limit_v_per_m;
     deterministic_ = config.deterministic != 0;
+    count_samples_ = config.count_samples != 0;
     auto const& p = config.propagation;
     propagation_.homogeneous = p.homogeneous_refractive_index;
     propagation_.min_height = p.minimum_height_m;
@@ -549,6 +552,7 @@ class Accumulator {
       double const factor = a == 1 ? s.sample_rate_hz : 1.;
       o.fixed_scale = deterministic_ ? kHeadroom * factor / limit_ : 1.;
       o.fixed_scale_f = static_cast<float>(o.fixed_scale);
+      o.count_samples = count_samples_ ? 1u : 0u;
       o.bins_d = static_cast<double>(s.number_of_bins);
       o.bins = s.number_of_bins;
       o.offset = offset;
@@ -643,7 +647,7 @@ class Accumulator {
       throw std::length_error("radio track capacity overflow");
     std::size_t const grown = capacity_ == 0 ? count : std::max(count, 2 * capacity_);
     if (capacity_ != 0) check(cudaStreamSynchronize(stream_), "grow fence");
-    tracks_.allocate(checked_mul(grown, kTrackRows));
+    tracks_.allocate(checked_mul(grown, kTrackDoubles));
     capacity_ = grown;
     stats_.track_workspace_bytes = tracks_.bytes();
     stats_.device_bytes = device_bytes();
@@ -746,7 +750,7 @@ class Accumulator {
   bool enabled_ = false;
   bool initialized_ = false;
   bool coreas_enabled_ = false, zhs_enabled_ = false, diagnostics_ = false;
-  bool fixed_ = true, deterministic_ = true, fuse_ = false;
+  bool fixed_ = true, deterministic_ = true, fuse_ = false, count_samples_ = false;
   bool downloaded_ = false, sealed_ = false, timing_ = false;
   int kernel_ = C8R_KERNEL_AUTO;
   Precision precision_ = Precision::kFP64;

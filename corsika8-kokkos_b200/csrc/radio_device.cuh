@@ -43,7 +43,7 @@ struct alignas(16) ObserverCache {
   double dest_integral;  // integratedRefractivity_[dest]              (:192)
   uint64_t dest_index;   // static_cast<size_t>(dest_height + 0.5)      (:187)
   float fixed_scale_f;
-  uint32_t pad_;
+  uint32_t count_samples;  // diagnostic: deposit 1 per component instead of the amplitude
 };
 
 // RadioPropagationView with the two tables interleaved as {n-1, integral}.
@@ -71,9 +71,11 @@ struct Track {
   double length, beta_module, constant;
 };
 
-// Structure-of-arrays track workspace: 14 rows of `capacity` doubles.
-enum TrackRow : int {
-  kSx = 0, kSy, kSz, kEx, kEy, kEz, kTs, kTe, kBx, kBy, kBz, kLen, kBmod, kConst, kTrackRows
+// Track workspace: one 128-byte record of 16 doubles per track (start xyz,
+// end xyz, t_start, t_end, beta xyz, length, |beta|, charge constant, two
+// spare), read by each thread with eight 16-byte vector loads.
+enum TrackField : int {
+  kSx = 0, kSy, kSz, kEx, kEy, kEz, kTs, kTe, kBx, kBy, kBz, kLen, kBmod, kConst, kTrackDoubles = 16
 };
 
 struct Path {

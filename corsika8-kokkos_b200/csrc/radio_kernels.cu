@@ -29,14 +29,22 @@ constexpr double kEmConstant = 1. / (4. * kPi * kVacuumPermittivity * kSpeedOfLi
 // ---------------------------------------------------------------- fixed point
 // add_radio_fixed_point, RadioProjection.inl:254-260.
 __device__ __forceinline__ bool to_fixed(double v, ObserverCache const& o, long long& out) {
+  if (o.count_samples) {
+    out = 1;
+    return true;
+  }
   double const s = v * o.fixed_scale;
-  if (!isfinite(s) || fabs(s) >= kSignedLimit) return false;
+  if (!(fabs(s) < kSignedLimit)) return false;  // also rejects NaN and infinities
   out = __double2ll_rn(s);
   return true;
 }
 __device__ __forceinline__ bool to_fixed(float v, ObserverCache const& o, long long& out) {
+  if (o.count_samples) {
+    out = 1;
+    return true;
+  }
   float const s = v * o.fixed_scale_f;
-  if (!isfinite(s) || fabsf(s) >= 9223372036854775808.f) return false;
+  if (!(fabsf(s) < 9223372036854775808.f)) return false;  // also rejects NaN and infinities
   out = __float2ll_rn(s);
   return true;
 }
@@ -56,6 +64,21 @@ __device__ __forceinline__ Vec3<T> scaled(Vec3<T> v, T s) {
   return {v.x * s, v.y * s, v.z * s};
 }
 
+// Signed overflow of the three adds previous + increment (two's complement),
+// the condition checked_radio_atomic_add tests; increments whose conversion
+// failed are passed as 0 and cannot overflow.
+__device__ __forceinline__ bool no_overflow3(unsigned long long px, long long x,
+                                             unsigned long long py, long long y,
+                                             unsigned long long pz, long long z) {
+  long long const sx = static_cast<long long>(px + static_cast<unsigned long long>(x));
+  long long const sy = static_cast<long long>(py + static_cast<unsigned long long>(y));
+  long long const sz = static_cast<long long>(pz + static_cast<unsigned long long>(z));
+  long long const bad = ((static_cast<long long>(px) ^ sx) & (x ^ sx)) |
+                        ((static_cast<long long>(py) ^ sy) & (y ^ sy)) |
+                        ((static_cast<long long>(pz) ^ sz) & (z ^ sz));
+  return bad >= 0;
+}
+
 // ---------------------------------------------------------------- sinks
 // Trace rows of one observer: global X|Y|Z rows already offset to the
 // observer's first bin.
@@ -66,7 +89,37 @@ struct GlobalSink {
     return checked(atomicAdd(row[c] + bin, static_cast<unsigned long long>(v)), v);
   }
   __device__ __forceinline__ void addf(int c, uint64_t bin, double v) { atomicAdd(frow[c] + bin, v); }
+  // All three components at one bin; false if a conversion failed or an add overflowed.
+  __device__ __forceinline__ bool add3(uint64_t bin, long long x, long long y, long long z,
+                                       bool ox, bool oy, bool oz) {
+    unsigned long long const px = ox ? atomicAdd(row[0] + bin, static_cast<unsigned long long>(x)) : 0ull;
+    unsigned long long const py = oy ? atomicAdd(row[1] + bin, static_cast<unsigned long long>(y)) : 0ull;
+    unsigned long long const pz = oz ? atomicAdd(row[2] + bin, static_cast<unsigned long long>(z)) : 0ull;
+    return ox && oy && oz && no_overflow3(px, x, py, y, pz, z);
+  }
+  __device__ __forceinline__ void addf3(uint64_t bin, double x, double y, double z) {
+    atomicAdd(frow[0] + bin, x);
+    atomicAdd(frow[1] + bin, y);
+    atomicAdd(frow[2] + bin, z);
+  }
 };
+
+// Bins past a shared-memory window: out of line, so the in-window path stays short.
+__device__ __noinline__ bool spill3(unsigned long long* r0, unsigned long long* r1,
+                                    unsigned long long* r2, long long x, long long y, long long z,
+                                    bool ox, bool oy, bool oz) {
+  unsigned long long const px = ox ? atomicAdd(r0, static_cast<unsigned long long>(x)) : 0ull;
+  unsigned long long const py = oy ? atomicAdd(r1, static_cast<unsigned long long>(y)) : 0ull;
+  unsigned long long const pz = oz ? atomicAdd(r2, static_cast<unsigned long long>(z)) : 0ull;
+  return ox && oy && oz && no_overflow3(px, x, py, y, pz, z);
+}
+
+__device__ __noinline__ void spillf3(double* r0, double* r1, double* r2, double x, double y,
+                                     double z) {
+  atomicAdd(r0, x);
+  atomicAdd(r1, y);
+  atomicAdd(r2, z);
+}
 
 // Shared-memory window of `width` bins starting at bin 0 (rows X|Y|Z), with
 // bins past the window spilled to the global rows.
@@ -87,6 +140,27 @@ struct WindowSink {
       atomicAdd(fwin + c * width + bin, v);
     else
       atomicAdd(frow[c] + bin, v);
+  }
+  __device__ __forceinline__ bool add3(uint64_t bin, long long x, long long y, long long z,
+                                       bool ox, bool oy, bool oz) {
+    if (bin >= width)
+      return spill3(row[0] + bin, row[1] + bin, row[2] + bin, x, y, z, ox, oy, oz);
+    unsigned long long* const w = win + bin;
+    unsigned long long const px = ox ? atomicAdd(w, static_cast<unsigned long long>(x)) : 0ull;
+    unsigned long long const py = oy ? atomicAdd(w + width, static_cast<unsigned long long>(y)) : 0ull;
+    unsigned long long const pz =
+        oz ? atomicAdd(w + 2 * width, static_cast<unsigned long long>(z)) : 0ull;
+    return ox && oy && oz && no_overflow3(px, x, py, y, pz, z);
+  }
+  __device__ __forceinline__ void addf3(uint64_t bin, double x, double y, double z) {
+    if (bin >= width) {
+      spillf3(frow[0] + bin, frow[1] + bin, frow[2] + bin, x, y, z);
+      return;
+    }
+    double* const w = fwin + bin;
+    atomicAdd(w, x);
+    atomicAdd(w + width, y);
+    atomicAdd(w + 2 * width, z);
   }
 };
 
@@ -130,17 +204,13 @@ __device__ __forceinline__ void deposit(ObserverCache const& o, Sink& sink, doub
   uint64_t bin;
   if (!sample_bin<kPotential>(o, t, bin)) return;
   if (kFixed) {
-    bool const ax = d.okx && sink.add(0, bin, d.ix);
-    bool const ay = d.oky && sink.add(1, bin, d.iy);
-    bool const az = d.okz && sink.add(2, bin, d.iz);
-    if (!(ax && ay && az)) {
+    if (!sink.add3(bin, d.okx ? d.ix : 0, d.oky ? d.iy : 0, d.okz ? d.iz : 0, d.okx, d.oky, d.okz)) {
       ++overflows;
       return;
     }
   } else {
-    sink.addf(0, bin, static_cast<double>(d.value.x));
-    sink.addf(1, bin, static_cast<double>(d.value.y));
-    sink.addf(2, bin, static_cast<double>(d.value.z));
+    sink.addf3(bin, static_cast<double>(d.value.x), static_cast<double>(d.value.y),
+               static_cast<double>(d.value.z));
   }
   ++contributions;
 }
@@ -152,18 +222,16 @@ __device__ __forceinline__ void add_sample(ObserverCache const& o, Sink& sink, d
   uint64_t bin;
   if (!sample_bin<kPotential>(o, t, bin)) return;
   if (kFixed) {
-    long long ix, iy, iz;
-    bool const ax = to_fixed(v.x, o, ix) && sink.add(0, bin, ix);
-    bool const ay = to_fixed(v.y, o, iy) && sink.add(1, bin, iy);
-    bool const az = to_fixed(v.z, o, iz) && sink.add(2, bin, iz);
-    if (!(ax && ay && az)) {
+    long long ix = 0, iy = 0, iz = 0;
+    bool const ox = to_fixed(v.x, o, ix);
+    bool const oy = to_fixed(v.y, o, iy);
+    bool const oz = to_fixed(v.z, o, iz);
+    if (!sink.add3(bin, ox ? ix : 0, oy ? iy : 0, oz ? iz : 0, ox, oy, oz)) {
       ++overflows;
       return;
     }
   } else {
-    sink.addf(0, bin, static_cast<double>(v.x));
-    sink.addf(1, bin, static_cast<double>(v.y));
-    sink.addf(2, bin, static_cast<double>(v.z));
+    sink.addf3(bin, static_cast<double>(v.x), static_cast<double>(v.y), static_cast<double>(v.z));
   }
   ++contributions;
 }
@@ -174,17 +242,13 @@ __device__ __forceinline__ void deposit_bin(Sink& sink, uint64_t bin, Deposit<Am
                                             unsigned long long& contributions,
                                             unsigned long long& overflows) {
   if (kFixed) {
-    bool const ax = d.okx && sink.add(0, bin, d.ix);
-    bool const ay = d.oky && sink.add(1, bin, d.iy);
-    bool const az = d.okz && sink.add(2, bin, d.iz);
-    if (!(ax && ay && az)) {
+    if (!sink.add3(bin, d.okx ? d.ix : 0, d.oky ? d.iy : 0, d.okz ? d.iz : 0, d.okx, d.oky, d.okz)) {
       ++overflows;
       return;
     }
   } else {
-    sink.addf(0, bin, static_cast<double>(d.value.x));
-    sink.addf(1, bin, static_cast<double>(d.value.y));
-    sink.addf(2, bin, static_cast<double>(d.value.z));
+    sink.addf3(bin, static_cast<double>(d.value.x), static_cast<double>(d.value.y),
+               static_cast<double>(d.value.z));
   }
   ++contributions;
 }
@@ -585,11 +649,14 @@ __device__ __forceinline__ void zhs_pair(Track const& t, Propagation const& p,
   // One segment when undivided: the loop below then evaluates
   // point2 = start + (end - start) / 1 / 1, exactly the reference's values.
   bool const subdivided = subtracks > 1 || refinement > 1;
-  double const rd = static_cast<double>(refinement);
-  double const rx = (t.ex - t.sx) / divisor / rd;
-  double const ry = (t.ey - t.sy) / divisor / rd;
-  double const rz = (t.ez - t.sz) / divisor / rd;
-  double const rt = (t.te - t.ts) / divisor / rd;
+  double rx = t.ex - t.sx, ry = t.ey - t.sy, rz = t.ez - t.sz, rt = t.te - t.ts;
+  if (subdivided) {  // x / 1 / 1 == x exactly, so undivided tracks skip the divisions
+    double const rd = static_cast<double>(refinement);
+    rx = rx / divisor / rd;
+    ry = ry / divisor / rd;
+    rz = rz / divisor / rd;
+    rt = rt / divisor / rd;
+  }
   double p1x = t.sx, p1y = t.sy, p1z = t.sz, t1 = t.ts;
   // subtrack-major, refinement-minor order of the reference's nested loops
   long long const segments = static_cast<long long>(subtracks) * refinement;
@@ -611,21 +678,25 @@ __device__ __forceinline__ void zhs_pair(Track const& t, Propagation const& p,
 // ---------------------------------------------------------------- helpers
 __device__ __forceinline__ Track load_track(const double* __restrict__ base, uint64_t stride,
                                             uint64_t i) {
+  (void)stride;
+  double2 const* r = reinterpret_cast<double2 const*>(base + i * kTrackDoubles);
+  double2 const a = __ldg(r + 0), b = __ldg(r + 1), c = __ldg(r + 2), d = __ldg(r + 3);
+  double2 const e = __ldg(r + 4), f = __ldg(r + 5), g = __ldg(r + 6);
   Track t;
-  t.sx = __ldg(base + kSx * stride + i);
-  t.sy = __ldg(base + kSy * stride + i);
-  t.sz = __ldg(base + kSz * stride + i);
-  t.ex = __ldg(base + kEx * stride + i);
-  t.ey = __ldg(base + kEy * stride + i);
-  t.ez = __ldg(base + kEz * stride + i);
-  t.ts = __ldg(base + kTs * stride + i);
-  t.te = __ldg(base + kTe * stride + i);
-  t.bx = __ldg(base + kBx * stride + i);
-  t.by = __ldg(base + kBy * stride + i);
-  t.bz = __ldg(base + kBz * stride + i);
-  t.length = __ldg(base + kLen * stride + i);
-  t.beta_module = __ldg(base + kBmod * stride + i);
-  t.constant = __ldg(base + kConst * stride + i);
+  t.sx = a.x;
+  t.sy = a.y;
+  t.sz = b.x;
+  t.ex = b.y;
+  t.ey = c.x;
+  t.ez = c.y;
+  t.ts = d.x;
+  t.te = d.y;
+  t.bx = e.x;
+  t.by = e.y;
+  t.bz = f.x;
+  t.length = f.y;
+  t.beta_module = g.x;
+  t.constant = g.y;
   return t;
 }
 
@@ -719,20 +790,15 @@ __global__ void __launch_bounds__(256) ingest_kernel(
   base = __shfl_sync(0xffffffffu, base, 0);
   if (valid) {
     uint64_t const j = base + __popc(ballot & ((1u << lane) - 1u));
-    tracks[kSx * stride + j] = t.sx;
-    tracks[kSy * stride + j] = t.sy;
-    tracks[kSz * stride + j] = t.sz;
-    tracks[kEx * stride + j] = t.ex;
-    tracks[kEy * stride + j] = t.ey;
-    tracks[kEz * stride + j] = t.ez;
-    tracks[kTs * stride + j] = t.ts;
-    tracks[kTe * stride + j] = t.te;
-    tracks[kBx * stride + j] = t.bx;
-    tracks[kBy * stride + j] = t.by;
-    tracks[kBz * stride + j] = t.bz;
-    tracks[kLen * stride + j] = t.length;
-    tracks[kBmod * stride + j] = t.beta_module;
-    tracks[kConst * stride + j] = t.constant;
+    double2* r = reinterpret_cast<double2*>(tracks + j * kTrackDoubles);
+    r[0] = make_double2(t.sx, t.sy);
+    r[1] = make_double2(t.sz, t.ex);
+    r[2] = make_double2(t.ey, t.ez);
+    r[3] = make_double2(t.ts, t.te);
+    r[4] = make_double2(t.bx, t.by);
+    r[5] = make_double2(t.bz, t.length);
+    r[6] = make_double2(t.beta_module, t.constant);
+    r[7] = make_double2(0., 0.);
   }
   if (lane == 0 && ballot) atomicAdd(&counters->valid_tracks, static_cast<unsigned long long>(__popc(ballot)));
   if (!diagnostics) return;
@@ -877,17 +943,12 @@ __device__ __forceinline__ void deposit_runs(Sink& sink, PendingRange const& run
     for (uint32_t k = lane; k < count; k += 32u) {
       uint64_t const bin = first + k;
       if (kFixed) {
-        bool const ax = sink.add(0, bin, vx);
-        bool const ay = sink.add(1, bin, vy);
-        bool const az = sink.add(2, bin, vz);
-        if (ax && ay && az)
+        if (sink.add3(bin, vx, vy, vz, true, true, true))
           ++c.zhs;
         else
           ++c.overflows;
       } else {
-        sink.addf(0, bin, __longlong_as_double(vx));
-        sink.addf(1, bin, __longlong_as_double(vy));
-        sink.addf(2, bin, __longlong_as_double(vz));
+        sink.addf3(bin, __longlong_as_double(vx), __longlong_as_double(vy), __longlong_as_double(vz));
         ++c.zhs;
       }
     }

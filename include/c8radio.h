@@ -126,6 +126,10 @@ typedef struct c8r_config {
   /* B200 extensions (zero keeps the defaults). */
   int32_t precision;          /* C8R_PRECISION_* */
   int32_t kernel;             /* C8R_KERNEL_* */
+  int32_t count_samples;      /* diagnostic: each in-range sample adds 1 to every
+                                 component instead of its amplitude (fixed-point
+                                 mode only); traces then count samples per bin */
+  int32_t reserved_;
 } c8r_config;
 
 /* corsika/kokkos/runtime/TuningParameters.hpp:14-21; zero keeps defaults.

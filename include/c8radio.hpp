@@ -53,6 +53,7 @@ struct RadioConfig {
   std::vector<RadioObserverSnapshot> zhsObservers_{};
   int precision_{C8R_PRECISION_FP64};
   int kernel_{C8R_KERNEL_AUTO};
+  bool countSamples_{};
 };
 
 // corsika/kokkos/runtime/TuningParameters.hpp:14-21
@@ -132,6 +133,7 @@ inline c8r_config view(RadioConfig const& c) {
   out.zhs_observer_count = c.zhsObservers_.size();
   out.precision = c.precision_;
   out.kernel = c.kernel_;
+  out.count_samples = c.countSamples_;
   return out;
 }
 

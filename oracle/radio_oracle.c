@@ -189,8 +189,12 @@ int c8o_checked_add(long long* address, long long increment) {
            (increment < 0 && previous < LLONG_MIN - increment));
 }
 
+/* Diagnostic sample-count mode of c8o_project: every in-range sample adds 1. */
+static int count_mode = 0;
+
 /* RadioProjection.inl:254-260. */
 int c8o_add_fixed_point(long long* address, double contribution, double scale) {
+  if (count_mode) return c8o_checked_add(address, 1);
   double scaled = contribution * scale;
   if (!isfinite(scaled) || fabs(scaled) >= kSignedLimit) return 0;
   return c8o_checked_add(address, (long long)rint(scaled));
@@ -611,6 +615,7 @@ int c8o_project(const c8r_config* config, const c8r_lepton_transport_record* rec
   propagation.table_size = p->table_size;
   propagation.zhs_subtrack_refinement = config->zhs_subtrack_refinement;
 
+  count_mode = config->count_samples != 0;
   if (threads <= 0) threads = 1;
 #ifndef _OPENMP
   threads = 1;
@@ -696,5 +701,6 @@ int c8o_project(const c8r_config* config, const c8r_lepton_transport_record* rec
   free(coreas_rows);
   free(zhs_rows);
   free(thread_counters);
+  count_mode = 0;
   return 0;
 }
