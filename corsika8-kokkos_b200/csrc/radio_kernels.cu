@@ -358,52 +358,53 @@ __device__ __noinline__ Counts coreas_pair_exact(Track const t, Propagation cons
   return c;
 }
 
-// Mixed-precision CoREAS pair.  Travel times, refractive indices and
-// distances are exact; emission directions are d * RN(1/|d|) (propagate's
+// The common CoREAS pair of the windowed kernel (RadioProjection.inl:339-409
+// without its near-Cherenkov branch).  Returns false, having deposited
+// nothing, when the pair needs the near-Cherenkov branch or (kFilter) an exact
+// evaluation; the kernel then defers it to coreas_pair_exact.
+//
+// kFilter (mixed precision): travel times, refractive indices and distances
+// are exact; emission directions are d * RN(1/|d|) (propagate's
 // kApproxDirection), so each Doppler factor 1 - n beta.k lies within
-// 14 u n |beta|_1 + 2 u of the reference's (u = 2^-53; bound below used with
-// a 4.5x margin).  The pair's branches (near-Cherenkov |doppler| < 1e-3, the
-// sign test doppler < 1e-9) are taken only when that bound cannot move them;
-// any pair closer than the bound to a threshold, or with |doppler| < 1e-6,
-// is evaluated exactly.  Sample times are exact, so bins are the reference's.
-template <bool kFixed, class Amp, class Sink>
-__device__ __forceinline__ void coreas_pair_filtered(Track const& t, Propagation const& p,
-                                                     ObserverCache const& o, Sink& sink,
-                                                     Counts& c) {
-  Path const ps = propagate<true, true>(p, o, t.sx, t.sy, t.sz);
-  Path const pe = propagate<true, true>(p, o, t.ex, t.ey, t.ez);
-  double const pre = 1. - ps.n_src * (t.bx * ps.kx + t.by * ps.ky + t.bz * ps.kz);
-  double const post = 1. - pe.n_src * (t.bx * pe.kx + t.by * pe.ky + t.bz * pe.kz);
-  double const beta1 = fabs(t.bx) + fabs(t.by) + fabs(t.bz) + 1.;
-  double const err_pre = ps.n_src * beta1 * 0x1p-47 + 0x1p-50;
-  double const err_post = pe.n_src * beta1 * 0x1p-47 + 0x1p-50;
-  bool const ambiguous =
-      fabs(pre) < 1.e-6 || fabs(post) < 1.e-6 ||
-      (ps.n_dst > 1. && (fabs(fabs(pre) - kCoreasThreshold) <= err_pre ||
-                         fabs(fabs(post) - kCoreasThreshold) <= err_post));
-  if (ambiguous) {
-    Counts const d = coreas_pair_exact<kFixed, Amp>(t, p, o, sink);
-    c.coreas += d.coreas;
-    c.overflows += d.overflows;
-    return;
+// 14 u n |beta|_1 + 2 u of the reference's (u = 2^-53; used below with a 4.5x
+// margin).  The branches (near-Cherenkov |doppler| < 1e-3, the sign test
+// doppler < 1e-9) are taken here only when that bound cannot move them, and
+// pairs with |doppler| < 1e-6 are left to the exact evaluation.  Sample times
+// are exact, so bins are the reference's.
+template <bool kFixed, bool kFilter, class Amp, class Sink>
+__device__ __forceinline__ bool coreas_common(Track const& t, Propagation const& p,
+                                              ObserverCache const& o, Sink& sink, Counts& c) {
+  Path const ps = propagate<true, kFilter>(p, o, t.sx, t.sy, t.sz);
+  Path const pe = propagate<true, kFilter>(p, o, t.ex, t.ey, t.ez);
+  double pre, post;
+  if (kFilter) {
+    pre = 1. - ps.n_src * (t.bx * ps.kx + t.by * ps.ky + t.bz * ps.kz);
+    post = 1. - pe.n_src * (t.bx * pe.kx + t.by * pe.ky + t.bz * pe.kz);
+    double const beta1 = fabs(t.bx) + fabs(t.by) + fabs(t.bz) + 1.;
+    double const err_pre = ps.n_src * beta1 * 0x1p-47 + 0x1p-50;
+    double const err_post = pe.n_src * beta1 * 0x1p-47 + 0x1p-50;
+    bool const ambiguous =
+        fabs(pre) < 1.e-6 || fabs(post) < 1.e-6 ||
+        (ps.n_dst > 1. && (fabs(fabs(pre) - kCoreasThreshold) <= err_pre ||
+                           fabs(fabs(post) - kCoreasThreshold) <= err_post));
+    if (ambiguous) return false;
+  } else {
+    pre = doppler(ps.n_src, t.bx, t.by, t.bz, ps.kx, ps.ky, ps.kz);
+    post = doppler(pe.n_src, t.bx, t.by, t.bz, pe.kx, pe.ky, pe.kz);
   }
+  if (ps.n_dst > 1. && (fabs(pre) < kCoreasThreshold || fabs(post) < kCoreasThreshold))
+    return false;
   double sr = t.ts + ps.time;
   double er = t.te + pe.time;
-  if (ps.n_dst > 1. && (fabs(pre) < kCoreasThreshold || fabs(post) < kCoreasThreshold)) {
-    Counts const d = coreas_near_cone<kFixed, Amp>(t, p, o, sink, sr < er);
-    c.coreas += d.coreas;
-    c.overflows += d.overflows;
-    return;
-  }
   Vec3<Amp> const beta{static_cast<Amp>(t.bx), static_cast<Amp>(t.by), static_cast<Amp>(t.bz)};
   Vec3<Amp> const ks{static_cast<Amp>(ps.kx), static_cast<Amp>(ps.ky), static_cast<Amp>(ps.kz)};
   Vec3<Amp> const ke{static_cast<Amp>(pe.kx), static_cast<Amp>(pe.ky), static_cast<Amp>(pe.kz)};
-  Amp const cf = static_cast<Amp>(t.constant * o.sample_rate);
+  double const cf = t.constant * o.sample_rate;
   Vec3<Amp> fstart =
-      scaled(cross(ks, cross(ks, beta)), amp_div(cf, static_cast<Amp>(pre * ps.dist)));
+      scaled(cross(ks, cross(ks, beta)), amp_div(static_cast<Amp>(cf), static_cast<Amp>(pre * ps.dist)));
   Vec3<Amp> fend =
-      scaled(cross(ke, cross(ke, beta)), amp_div(-cf, static_cast<Amp>(post * pe.dist)));
-  // |pre|, |post| >= 1e-6 here, so "< 1e-9" is the sign of the factor
+      scaled(cross(ke, cross(ke, beta)), amp_div(static_cast<Amp>(-cf), static_cast<Amp>(post * pe.dist)));
+  // with the filter |pre|, |post| >= 1e-6, so "< 1e-9" is the sign of the factor
   if (pre < 1.e-9 || post < 1.e-9) {
     double const res = o.resolution;
     double const dt = er - sr;
@@ -416,6 +417,7 @@ __device__ __forceinline__ void coreas_pair_filtered(Track const& t, Propagation
   }
   add_sample<false, kFixed>(o, sink, sr, fstart, c.coreas, c.overflows);
   add_sample<false, kFixed>(o, sink, er, fend, c.coreas, c.overflows);
+  return true;
 }
 
 // Intermediate ZHS bins binned index by index with the reference's own
@@ -444,13 +446,6 @@ __device__ __noinline__ Counts zhs_indexed_bins(ObserverCache const& o, Sink sin
 }
 
 // ---------------------------------------------------------------- ZHS
-template <bool kFixed, class Amp, class Sink>
-__device__ __noinline__ Counts zhs_segment_exact(double p1x, double p1y, double p1z, double p2x,
-                                                 double p2y, double p2z, double t1, double t2,
-                                                 Track const t, Propagation const& p,
-                                                 ObserverCache const& o, Sink sink,
-                                                 bool subdivided);
-
 // accumulate_zhs_segment, RadioProjection.inl:412-480.
 //
 // kRuns = true (windowed kernel): the intermediate bins of a segment are the
@@ -465,9 +460,10 @@ __device__ __noinline__ Counts zhs_segment_exact(double p1x, double p1y, double 
 // time within e_d; every decision the segment takes (which detection time is
 // first, the nearest bin and floor(x + 0.5) of both, |1 - n beta.k| > 1e-15,
 // the consecutive-run test) is taken only when those bounds cannot change it,
-// else the segment is evaluated exactly.  Bins and counts are the reference's.
+// else the segment returns false having deposited nothing (the caller then
+// evaluates it exactly).  Bins and counts are the reference's.
 template <bool kFixed, bool kRuns, bool kFilter, class Amp, class Sink>
-__device__ __forceinline__ void zhs_segment(double p1x, double p1y, double p1z, double p2x,
+__device__ __forceinline__ bool zhs_segment(double p1x, double p1y, double p1z, double p2x,
                                             double p2y, double p2z, double t1, double t2,
                                             Track const& t, Propagation const& p,
                                             ObserverCache const& o, Sink& sink, Counts& c,
@@ -520,13 +516,7 @@ __device__ __forceinline__ void zhs_segment(double p1x, double p1y, double p1z, 
     bool const ambiguous = fabs(d1 - d2) <= 2. * e_d || fabs(den) < 1.e-6 ||
                            f1 <= e_x + 0x1p-50 * (fabs(x1) + 1.) ||
                            f2 <= e_x + 0x1p-50 * (fabs(x2) + 1.) || (nb > 1 && !run_ok);
-    if (ambiguous) {
-      Counts const d = zhs_segment_exact<kFixed, Amp>(p1x, p1y, p1z, p2x, p2y, p2z, t1, t2, t, p,
-                                                      o, sink, subdivided);
-      c.zhs += d.zhs;
-      c.overflows += d.overflows;
-      return;
-    }
+    if (ambiguous) return false;
   }
   Vec3<Amp> const k{static_cast<Amp>(path.kx), static_cast<Amp>(path.ky), static_cast<Amp>(path.kz)};
   Vec3<Amp> const beta{static_cast<Amp>(t.bx), static_cast<Amp>(t.by), static_cast<Amp>(t.bz)};
@@ -545,7 +535,7 @@ __device__ __forceinline__ void zhs_segment(double p1x, double p1y, double p1z, 
                            scaled(perp, amp_div(static_cast<Amp>(sc * frac_last),
                                                 static_cast<Amp>(den_last))),
                            c.zhs, c.overflows);
-  if (single) return;
+  if (single) return true;
   double const frac_first = fabs(sb + 0.5 - x1);
   add_sample<true, kFixed>(o, sink, d1,
                            scaled(perp, amp_div(static_cast<Amp>(sc * frac_first), static_cast<Amp>(dd))),
@@ -587,62 +577,24 @@ __device__ __forceinline__ void zhs_segment(double p1x, double p1y, double p1z, 
       c.overflows += d.overflows;
     }
   }
+  return true;
 }
 
-// The exact segment out of line: the filtered path's fallback.
-template <bool kFixed, class Amp, class Sink>
-__device__ __noinline__ Counts zhs_segment_exact(double p1x, double p1y, double p1z, double p2x,
-                                                 double p2y, double p2z, double t1, double t2,
-                                                 Track const t, Propagation const& p,
-                                                 ObserverCache const& o, Sink sink,
-                                                 bool subdivided) {
-  Counts c;
-  zhs_segment<kFixed, true, false, Amp>(p1x, p1y, p1z, p2x, p2y, p2z, t1, t2, t, p, o, sink, c,
-                                        subdivided, nullptr);
-  return c;
-}
-
-// accumulate_zhs, RadioProjection.inl:483-529.
-//
-// kFilter: the Fraunhofer number F is first estimated in FP32 as
-// sin^2(theta) K with sin^2 = |beta x d|^2 / (|beta|^2 |d|^2) and
-// K = 2 pi L^2 / (|d| lambda); its distance from the reference's FP64 F is at
-// most 1.7e-6 sqrt(K F) + 1e-6 F + 1e-12 K (cross-product cancellation and
-// the FP32 roundings; used with a 4x margin).  When the estimate lies surely
-// below 1 the track is one undivided segment, exactly as the reference
-// decides; otherwise F is evaluated exactly.
-template <bool kFixed, bool kRuns, bool kFilter, class Amp, class Sink>
+// accumulate_zhs, RadioProjection.inl:483-529, every decision exact.
+template <bool kFixed, bool kRuns, class Amp, class Sink>
 __device__ __forceinline__ void zhs_pair(Track const& t, Propagation const& p,
                                          ObserverCache const& o, Sink& sink, Counts& c,
                                          PendingRange* pending) {
   double const mx = (t.sx + t.ex) * 0.5, my = (t.sy + t.ey) * 0.5, mz = (t.sz + t.ez) * 0.5;
+  Path const pm = propagate<false>(p, o, mx, my, mz);
+  double const uk = (t.bx * pm.kx + t.by * pm.ky + t.bz * pm.kz) / t.beta_module;
+  double const s2 = 1. - uk * uk;
+  double const fraunhofer = s2 * t.length * t.length / pm.dist / o.wavelength * 2. * kPi;
   double divisor = 1.;
   int subtracks = 1;
-  bool exact_fraunhofer = true;
-  if (kFilter) {
-    float const dx = static_cast<float>(o.px - mx), dy = static_cast<float>(o.py - my),
-                dz = static_cast<float>(o.pz - mz);
-    float const bx = static_cast<float>(t.bx), by = static_cast<float>(t.by),
-                bz = static_cast<float>(t.bz);
-    float const cx = by * dz - bz * dy, cy = bz * dx - bx * dz, cz = bx * dy - by * dx;
-    float const d2 = dx * dx + dy * dy + dz * dz;
-    float const b2 = bx * bx + by * by + bz * bz;
-    float const length = static_cast<float>(t.length);
-    float const s2 = (cx * cx + cy * cy + cz * cz) / (b2 * d2);
-    float const k = 6.2831853f * length * length / (sqrtf(d2) * static_cast<float>(o.wavelength));
-    float const f = s2 * k;
-    float const margin = 4.e-6f * sqrtf(k * (f + 1.f)) + 4.e-5f * (f + 1.f) + 4.e-12f * k;
-    exact_fraunhofer = !(f + margin < 1.f);
-  }
-  if (exact_fraunhofer) {
-    Path const pm = propagate<false>(p, o, mx, my, mz);
-    double const uk = (t.bx * pm.kx + t.by * pm.ky + t.bz * pm.kz) / t.beta_module;
-    double const s2 = 1. - uk * uk;
-    double const fraunhofer = s2 * t.length * t.length / pm.dist / o.wavelength * 2. * kPi;
-    if (fraunhofer > 1.) {
-      divisor = sqrt(fraunhofer) + 1.;
-      subtracks = x86_int(ceil(divisor));
-    }
+  if (fraunhofer > 1.) {
+    divisor = sqrt(fraunhofer) + 1.;
+    subtracks = x86_int(ceil(divisor));
   }
   c.subtracks += static_cast<unsigned long long>(static_cast<long long>(subtracks));
   int const refinement = static_cast<int>(p.refinement);
@@ -663,8 +615,8 @@ __device__ __forceinline__ void zhs_pair(Track const& t, Propagation const& p,
 #pragma unroll 1
   for (long long index = 0; index < segments; ++index) {
     double const p2x = p1x + rx, p2y = p1y + ry, p2z = p1z + rz, t2 = t1 + rt;
-    zhs_segment<kFixed, kRuns, kFilter, Amp>(p1x, p1y, p1z, p2x, p2y, p2z, t1, t2, t, p, o, sink,
-                                             c, subdivided, pending);
+    zhs_segment<kFixed, kRuns, false, Amp>(p1x, p1y, p1z, p2x, p2y, p2z, t1, t2, t, p, o, sink, c,
+                                           subdivided, pending);
     p1x = p2x;
     p1y = p2y;
     p1z = p2z;
@@ -673,6 +625,63 @@ __device__ __forceinline__ void zhs_pair(Track const& t, Propagation const& p,
   if (refinement > 1)
     c.subtracks += static_cast<unsigned long long>(
         static_cast<long long>(subtracks * (refinement - 1)));
+}
+
+// The exact pair out of line: deferred ZHS pairs of the windowed kernel.
+template <bool kFixed, class Amp, class Sink>
+__device__ __noinline__ Counts zhs_pair_exact(Track const t, Propagation const& p,
+                                              ObserverCache const& o, Sink sink) {
+  Counts c;
+  zhs_pair<kFixed, true, Amp>(t, p, o, sink, c, nullptr);
+  return c;
+}
+
+// The common ZHS pair of the windowed kernel: one undivided segment.  Returns
+// false, having deposited nothing, when the track is subdivided (Fraunhofer
+// number above 1, or refinement), when (kFilter) the Fraunhofer test is not
+// surely below 1, or when the filtered segment is ambiguous; the kernel then
+// defers the pair to zhs_pair_exact.
+//
+// kFilter: F is estimated in FP32 as sin^2(theta) K with
+// sin^2 = |beta x d|^2 / (|beta|^2 |d|^2) and K = 2 pi L^2 / (|d| lambda); its
+// distance from the reference's FP64 F is at most 1.7e-6 sqrt(K F) + 1e-6 F +
+// 1e-12 K (cross-product cancellation and the FP32 roundings; used with a 4x
+// margin), so an estimate surely below 1 decides "one segment" exactly as the
+// reference does.
+template <bool kFixed, bool kFilter, class Amp, class Sink>
+__device__ __forceinline__ bool zhs_common(Track const& t, Propagation const& p,
+                                           ObserverCache const& o, Sink& sink, Counts& c,
+                                           PendingRange* pending) {
+  if (p.refinement != 1u) return false;
+  double const mx = (t.sx + t.ex) * 0.5, my = (t.sy + t.ey) * 0.5, mz = (t.sz + t.ez) * 0.5;
+  if (kFilter) {
+    float const dx = static_cast<float>(o.px - mx), dy = static_cast<float>(o.py - my),
+                dz = static_cast<float>(o.pz - mz);
+    float const bx = static_cast<float>(t.bx), by = static_cast<float>(t.by),
+                bz = static_cast<float>(t.bz);
+    float const cx = by * dz - bz * dy, cy = bz * dx - bx * dz, cz = bx * dy - by * dx;
+    float const d2 = dx * dx + dy * dy + dz * dz;
+    float const b2 = bx * bx + by * by + bz * bz;
+    float const length = static_cast<float>(t.length);
+    float const s2 = (cx * cx + cy * cy + cz * cz) / (b2 * d2);
+    float const k = 6.2831853f * length * length / (sqrtf(d2) * static_cast<float>(o.wavelength));
+    float const f = s2 * k;
+    float const margin = 4.e-6f * sqrtf(k * (f + 1.f)) + 4.e-5f * (f + 1.f) + 4.e-12f * k;
+    if (!(f + margin < 1.f)) return false;
+  } else {
+    Path const pm = propagate<false>(p, o, mx, my, mz);
+    double const uk = (t.bx * pm.kx + t.by * pm.ky + t.bz * pm.kz) / t.beta_module;
+    double const s2 = 1. - uk * uk;
+    double const fraunhofer = s2 * t.length * t.length / pm.dist / o.wavelength * 2. * kPi;
+    if (fraunhofer > 1.) return false;
+  }
+  if (!zhs_segment<kFixed, true, kFilter, Amp>(t.sx, t.sy, t.sz, t.sx + (t.ex - t.sx),
+                                               t.sy + (t.ey - t.sy), t.sz + (t.ez - t.sz), t.ts,
+                                               t.ts + (t.te - t.ts), t, p, o, sink, c, false,
+                                               pending))
+    return false;
+  c.subtracks += 1ull;
+  return true;
 }
 
 // ---------------------------------------------------------------- helpers
@@ -917,7 +926,7 @@ __global__ void __launch_bounds__(256) direct_kernel(const __grid_constant__ Eve
         sink.row[r] = kFixed ? ev.fixed[1] + r * ev.total_bins[1] + o.offset : nullptr;
         sink.frow[r] = kFixed ? nullptr : ev.floating[1] + r * ev.total_bins[1] + o.offset;
       }
-      zhs_pair<kFixed, false, false, Amp>(t, ev.propagation, o, sink, c, nullptr);
+      zhs_pair<kFixed, false, Amp>(t, ev.propagation, o, sink, c, nullptr);
     }
   }
   flush_counts(c, ev.counters);
@@ -925,6 +934,7 @@ __global__ void __launch_bounds__(256) direct_kernel(const __grid_constant__ Eve
 
 // ---------------------------------------------------------------- windowed
 constexpr int kWindowThreadsMax = 512;
+constexpr unsigned kWarpQueue = 64;  // entries per warp: < 32 kept + 32 pushed per round
 
 // Each lane's pending run of consecutive ZHS bins is deposited by the whole
 // warp, 32 bins per step.  Every lane of the warp must call it.
@@ -1009,26 +1019,51 @@ __global__ void __launch_bounds__(kWindowThreadsMax, 1)
       sink.frow[row] = kFixed ? nullptr : ev.floating[algorithm] + row * total + o.offset;
     }
     constexpr bool kFilter = sizeof(Amp) == sizeof(float);  // mixed precision
-    if (kAlgorithm == 0) {
-      for (uint64_t i = begin + threadIdx.x; i < end; i += blockDim.x) {
-        if (kFilter)
-          coreas_pair_filtered<kFixed, Amp>(load_track(ev.tracks, ev.stride, i), ev.propagation, o,
-                                            sink, c);
-        else
-          coreas_pair<kFixed, Amp>(load_track(ev.tracks, ev.stride, i), ev.propagation, o, sink, c);
+    // Per-warp queue of deferred pairs (track offsets in the chunk): pairs that
+    // need the near-Cherenkov branch, an exact evaluation or a subdivided
+    // track.  A warp drains 32 of them at a time, converged, with the exact
+    // code, so rare paths do not hold up the common path of the other lanes.
+    unsigned* const queue =
+        reinterpret_cast<unsigned*>(window + 3 * static_cast<size_t>(plan.window)) +
+        (threadIdx.x >> 5) * kWarpQueue;
+    unsigned const lane = threadIdx.x & 31u;
+    unsigned queued = 0;  // warp-uniform
+    auto drain = [&](unsigned from, unsigned count) {
+      if (lane < count) {
+        Track const t = load_track(ev.tracks, ev.stride, begin + queue[from + lane]);
+        Counts const d = kAlgorithm == 0 ? coreas_pair_exact<kFixed, Amp>(t, ev.propagation, o, sink)
+                                         : zhs_pair_exact<kFixed, Amp>(t, ev.propagation, o, sink);
+        c.coreas += d.coreas;
+        c.zhs += d.zhs;
+        c.subtracks += d.subtracks;
+        c.overflows += d.overflows;
       }
-    } else {
-      // uniform trip count: every warp reaches deposit_runs converged
-      for (uint64_t base = begin; base < end; base += blockDim.x) {
-        uint64_t const i = base + threadIdx.x;
-        PendingRange run;
-        run.count = 0;
-        if (i < end)
-          zhs_pair<kFixed, true, kFilter, Amp>(load_track(ev.tracks, ev.stride, i),
-                                               ev.propagation, o, sink, c, &run);
-        deposit_runs<kFixed>(sink, run, c);
+      __syncwarp();
+    };
+    for (uint64_t base = begin; base < end; base += blockDim.x) {
+      uint64_t const i = base + threadIdx.x;
+      bool deferred = false;
+      PendingRange run;
+      run.count = 0;
+      if (i < end) {
+        Track const t = load_track(ev.tracks, ev.stride, i);
+        bool const done =
+            kAlgorithm == 0 ? coreas_common<kFixed, kFilter, Amp>(t, ev.propagation, o, sink, c)
+                            : zhs_common<kFixed, kFilter, Amp>(t, ev.propagation, o, sink, c, &run);
+        deferred = !done;
+      }
+      if (kAlgorithm == 1) deposit_runs<kFixed>(sink, run, c);
+      unsigned const ballot = __ballot_sync(0xffffffffu, deferred);
+      if (deferred)
+        queue[queued + __popc(ballot & ((1u << lane) - 1u))] = static_cast<unsigned>(i - begin);
+      queued += __popc(ballot);
+      __syncwarp();
+      if (queued >= 32u) {
+        queued -= 32u;
+        drain(queued, 32u);
       }
     }
+    if (queued) drain(0u, queued);
     __syncthreads();
 
     // flush: non-zero bins, checked global adds
@@ -1086,10 +1121,15 @@ cudaError_t direct_dispatch(EventPlan const& ev, uint64_t bound, bool coreas, bo
   return cudaGetLastError();
 }
 
+size_t windowed_smem_bytes(uint32_t window) {
+  return static_cast<size_t>(window) * 3 * sizeof(unsigned long long) +
+         (kWindowThreadsMax / 32) * kWarpQueue * sizeof(unsigned);
+}
+
 template <bool kFixed, class Amp, int kAlgorithm>
 cudaError_t windowed_dispatch_algorithm(WorkPlan const& plan, int ctas, int threads,
                                         cudaStream_t stream) {
-  size_t const bytes = static_cast<size_t>(plan.window) * 3 * sizeof(unsigned long long);
+  size_t const bytes = windowed_smem_bytes(plan.window);
   cudaError_t err = cudaFuncSetAttribute(windowed_kernel<kFixed, Amp, kAlgorithm>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(bytes));
@@ -1107,7 +1147,7 @@ cudaError_t windowed_dispatch(WorkPlan const& plan, int ctas, int threads, cudaS
 
 template <bool kFixed, class Amp>
 int ctas_per_sm(int window, int threads) {
-  size_t const bytes = static_cast<size_t>(window) * 3 * sizeof(unsigned long long);
+  size_t const bytes = windowed_smem_bytes(static_cast<uint32_t>(window));
   int worst = 1 << 30;
   auto probe = [&](auto kernel) {
     cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
@@ -1158,8 +1198,8 @@ cudaError_t launch_windowed(WorkPlan const& plan, bool fixed, Precision precisio
 int windowed_max_bins(int device) {
   int optin = 0;
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
-  // static shared memory of the kernel is a handful of bytes; keep 1 KiB spare
-  int const usable = optin - 1024;
+  // static shared memory of the kernel is a few hundred bytes; keep 1 KiB spare
+  int const usable = optin - 1024 - static_cast<int>((kWindowThreadsMax / 32) * kWarpQueue * sizeof(unsigned));
   return usable > 0 ? usable / static_cast<int>(3 * sizeof(unsigned long long)) : 0;
 }
 
