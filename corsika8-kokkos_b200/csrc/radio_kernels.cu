@@ -446,6 +446,61 @@ __device__ __noinline__ Counts zhs_indexed_bins(ObserverCache const& o, Sink sin
 }
 
 // ---------------------------------------------------------------- ZHS
+// The multi-bin tail of a ZHS segment (first sample and intermediate bins,
+// RadioProjection.inl:457-472), out of line: about half the segments take it,
+// and keeping it out of the common path saves registers and instruction fetch.
+// A run of intermediate bins left for the warp is returned in `run` when
+// want_run.
+template <bool kFixed, bool kRuns, class Amp, class Sink>
+__device__ __noinline__ Counts zhs_multi_tail(ObserverCache const& o, Sink sink, double d1,
+                                              double x1, double sb, int nb, Vec3<Amp> perp,
+                                              double sc, double dd, double mc, bool run_ok,
+                                              bool want_run, PendingRange& run) {
+  Counts c;
+  PendingRange* pending = want_run ? &run : nullptr;
+  double const frac_first = fabs(sb + 0.5 - x1);
+  add_sample<true, kFixed>(o, sink, d1,
+                           scaled(perp, amp_div(static_cast<Amp>(sc * frac_first), static_cast<Amp>(dd))),
+                           c.zhs, c.overflows);
+  if (nb > 1) {
+    Deposit<Amp> const mid =
+        make_deposit<kFixed>(o, scaled(perp, amp_div(static_cast<Amp>(mc), static_cast<Amp>(dd))));
+    if (kRuns && run_ok) {
+      long long const b1 = static_cast<long long>(floor(x1)) + (x1 - floor(x1) >= 0.5 ? 1 : 0);
+      long long lo = 1, hi = nb;
+      if (-b1 > lo) lo = -b1;
+      long long const top = static_cast<long long>(o.bins) - b1;
+      if (top < hi) hi = top;
+      if (hi > lo) {
+        uint64_t const first = static_cast<uint64_t>(b1 + lo);
+        uint32_t const count = static_cast<uint32_t>(hi - lo);
+        bool const all_ok = !kFixed || (mid.okx && mid.oky && mid.okz);
+        if (pending && all_ok && count >= kCooperativeRun && pending->count == 0) {
+          pending->bin = first;
+          pending->count = count;
+          if (kFixed) {
+            pending->v[0] = mid.ix;
+            pending->v[1] = mid.iy;
+            pending->v[2] = mid.iz;
+          } else {
+            pending->v[0] = __double_as_longlong(static_cast<double>(mid.value.x));
+            pending->v[1] = __double_as_longlong(static_cast<double>(mid.value.y));
+            pending->v[2] = __double_as_longlong(static_cast<double>(mid.value.z));
+          }
+        } else {
+          for (uint32_t j = 0; j < count; ++j)
+            deposit_bin<kFixed>(sink, first + j, mid, c.zhs, c.overflows);
+        }
+      }
+    } else {
+      Counts const d = zhs_indexed_bins<kFixed, Amp>(o, sink, d1, x1, nb, mid);
+      c.zhs += d.zhs;
+      c.overflows += d.overflows;
+    }
+  }
+  return c;
+}
+
 // accumulate_zhs_segment, RadioProjection.inl:412-480.
 //
 // kRuns = true (windowed kernel): the intermediate bins of a segment are the
@@ -536,47 +591,14 @@ __device__ __forceinline__ bool zhs_segment(double p1x, double p1y, double p1z, 
                                                 static_cast<Amp>(den_last))),
                            c.zhs, c.overflows);
   if (single) return true;
-  double const frac_first = fabs(sb + 0.5 - x1);
-  add_sample<true, kFixed>(o, sink, d1,
-                           scaled(perp, amp_div(static_cast<Amp>(sc * frac_first), static_cast<Amp>(dd))),
-                           c.zhs, c.overflows);
-  if (nb > 1) {
-    double const mc = (subdivided ? 1. : sign) * t.constant;
-    Deposit<Amp> const mid =
-        make_deposit<kFixed>(o, scaled(perp, amp_div(static_cast<Amp>(mc), static_cast<Amp>(dd))));
-    if (kRuns && run_ok) {
-      long long const b1 = static_cast<long long>(floor(x1)) + (x1 - floor(x1) >= 0.5 ? 1 : 0);
-      long long lo = 1, hi = nb;
-      if (-b1 > lo) lo = -b1;
-      long long const top = static_cast<long long>(o.bins) - b1;
-      if (top < hi) hi = top;
-      if (hi > lo) {
-        uint64_t const first = static_cast<uint64_t>(b1 + lo);
-        uint32_t const count = static_cast<uint32_t>(hi - lo);
-        bool const all_ok = !kFixed || (mid.okx && mid.oky && mid.okz);
-        if (pending && all_ok && count >= kCooperativeRun && pending->count == 0) {
-          pending->bin = first;
-          pending->count = count;
-          if (kFixed) {
-            pending->v[0] = mid.ix;
-            pending->v[1] = mid.iy;
-            pending->v[2] = mid.iz;
-          } else {
-            pending->v[0] = __double_as_longlong(static_cast<double>(mid.value.x));
-            pending->v[1] = __double_as_longlong(static_cast<double>(mid.value.y));
-            pending->v[2] = __double_as_longlong(static_cast<double>(mid.value.z));
-          }
-        } else {
-          for (uint32_t j = 0; j < count; ++j)
-            deposit_bin<kFixed>(sink, first + j, mid, c.zhs, c.overflows);
-        }
-      }
-    } else {
-      Counts const d = zhs_indexed_bins<kFixed, Amp>(o, sink, d1, x1, nb, mid);
-      c.zhs += d.zhs;
-      c.overflows += d.overflows;
-    }
-  }
+  PendingRange run;
+  run.count = 0;
+  Counts const d = zhs_multi_tail<kFixed, kRuns, Amp>(
+      o, sink, d1, x1, sb, nb, perp, sc, dd, (subdivided ? 1. : sign) * t.constant, run_ok,
+      pending != nullptr && pending->count == 0, run);
+  c.zhs += d.zhs;
+  c.overflows += d.overflows;
+  if (run.count) *pending = run;
   return true;
 }
 
@@ -934,6 +956,9 @@ __global__ void __launch_bounds__(256) direct_kernel(const __grid_constant__ Eve
 
 // ---------------------------------------------------------------- windowed
 constexpr int kWindowThreadsMax = 512;
+// The ZHS kernel's live state needs more than 128 registers a thread: it runs
+// 384-thread CTAs (up to 168 registers, no spills).
+constexpr int kZhsThreadsMax = 384;
 constexpr unsigned kWarpQueue = 64;  // entries per warp: < 32 kept + 32 pushed per round
 
 // Each lane's pending run of consecutive ZHS bins is deposited by the whole
@@ -978,7 +1003,7 @@ __device__ __forceinline__ uint32_t find_event(EventPlan const* events, uint32_t
 }
 
 template <bool kFixed, class Amp, int kAlgorithm>
-__global__ void __launch_bounds__(kWindowThreadsMax, 1)
+__global__ void __launch_bounds__(kAlgorithm == 1 ? kZhsThreadsMax : kWindowThreadsMax, 1)
     windowed_kernel(const __grid_constant__ WorkPlan plan) {
   extern __shared__ __align__(16) unsigned long long window[];
   __shared__ unsigned long long item_shared;
@@ -1134,7 +1159,8 @@ cudaError_t windowed_dispatch_algorithm(WorkPlan const& plan, int ctas, int thre
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(bytes));
   if (err != cudaSuccess) return err;
-  windowed_kernel<kFixed, Amp, kAlgorithm><<<ctas, threads, bytes, stream>>>(plan);
+  int const block = kAlgorithm == 1 && threads > kZhsThreadsMax ? kZhsThreadsMax : threads;
+  windowed_kernel<kFixed, Amp, kAlgorithm><<<ctas, block, bytes, stream>>>(plan);
   return cudaGetLastError();
 }
 
@@ -1149,15 +1175,15 @@ template <bool kFixed, class Amp>
 int ctas_per_sm(int window, int threads) {
   size_t const bytes = windowed_smem_bytes(static_cast<uint32_t>(window));
   int worst = 1 << 30;
-  auto probe = [&](auto kernel) {
+  auto probe = [&](auto kernel, int block) {
     cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
     int blocks = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, threads, bytes) != cudaSuccess)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, block, bytes) != cudaSuccess)
       blocks = 0;
     worst = blocks < worst ? blocks : worst;
   };
-  probe(windowed_kernel<kFixed, Amp, 0>);
-  probe(windowed_kernel<kFixed, Amp, 1>);
+  probe(windowed_kernel<kFixed, Amp, 0>, threads);
+  probe(windowed_kernel<kFixed, Amp, 1>, threads > kZhsThreadsMax ? kZhsThreadsMax : threads);
   return worst;
 }
 
