@@ -43,6 +43,7 @@ FLOP_COREAS_PAIR = 108 + 14   # two propagations, two Doppler factors, two field
 FLOP_ZHS_SETUP = 40 + 12      # Fraunhofer midpoint propagation and subdivision
 FLOP_ZHS_SUBTRACK = 79 + 7    # one segment: propagation, detection times, potential
 FLOP_SAMPLE = 12 + 3          # bin, gate and three fixed-point conversions
+TRACK_BYTES = 128             # algorithmic read per track per launch (packed kinematics)
 
 WORKLOAD_NAME = "tiled_c1"
 
@@ -132,6 +133,13 @@ def build_workload(name: str, segments: int, seed: int):
     else:
         records = showers.shower_records(n, seed=seed, **gen)
     return pkg, showers, wl, records
+
+
+def hbm_peak_gbs():
+    path = ROOT / "MEASURED_PEAKS.json"
+    if path.exists():
+        return json.loads(path.read_text()).get("hbm_gbs")
+    return 6650.0  # fallback figure for this pool's B200s
 
 
 def algorithmic_flops(pairs: int, counters: dict) -> float:
@@ -258,22 +266,46 @@ def run_ours(args):
             variants[label] = {"pairs_per_s": pairs_per_step / (vms * 1e-3), "ms_per_step": vms,
                                "kernel_ms": vkms, "clocks_sm_mhz": vclocks.get("sm_mhz")}
 
-    # roofline of the projection kernel (per launch = per step)
-    flops = algorithmic_flops(pairs_per_step, {k: counters[k] / args.steps for k in
-                                               ("zhs_subtracks", "coreas_contributions",
-                                                "zhs_contributions")})
-    achieved = flops / (kernel_ms * 1e-3) / 1e12
+    # roofline of the dominant kernel (the windowed ZHS launch, two thirds of a
+    # step) and of the CoREAS launch, from events on their launch stream
+    per = {k: counters[k] / args.steps for k in ("zhs_subtracks", "coreas_contributions",
+                                                  "zhs_contributions")}
+    zhs_flops = (pairs_per_step * FLOP_ZHS_SETUP + per["zhs_subtracks"] * FLOP_ZHS_SUBTRACK +
+                 per["zhs_contributions"] * FLOP_SAMPLE)
+    coreas_flops = pairs_per_step * FLOP_COREAS_PAIR + per["coreas_contributions"] * FLOP_SAMPLE
+    zhs_ms = stats.zhs_kernel_time_ms / args.steps
+    coreas_ms = stats.coreas_kernel_time_ms / args.steps
     peak = peaks["fp64_flops"] / 1e12
-    roofline = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                "frac": achieved / peak if peak else None, "traffic": None,
-                "peak_source": "FP64 FMA stream measured in this run (c8r_probe_peaks)",
-                "kernel": "windowed_kernel (projection)", "kernel_ms": kernel_ms,
-                "flop_per_launch": flops,
-                "atomics": {"shared_per_s_peak": peaks["shared_atomics_per_s"],
-                            "global_per_s_peak": peaks["global_atomics_per_s"],
-                            "samples_per_s": (counters["coreas_contributions"] +
-                                              counters["zhs_contributions"]) / args.steps /
-                                             (kernel_ms * 1e-3)}}
+    traffic = {}
+    traffic_file = ROOT / "profiles" / "windowed_traffic.json"
+    if traffic_file.exists():
+        t = json.loads(traffic_file.read_text())
+        traffic = {"zhs": t["zhs_bytes_per_track"] * n, "coreas": t["coreas_bytes_per_track"] * n}
+
+    def roof(flops, ms, key):
+        achieved = flops / (ms * 1e-3) / 1e12 if ms > 0 else None
+        return {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak if achieved and peak else None,
+                "traffic": traffic.get(key), "kernel_ms": ms, "flop_per_launch": flops,
+                "bytes_per_launch_algorithmic": TRACK_BYTES * n}
+
+    roofline = roof(zhs_flops, zhs_ms, "zhs")
+    roofline.update({
+        "kernel": "windowed_kernel<fixed,float,ZHS> (dominant, 2/3 of the step)",
+        "peak_source": "FP64 FMA stream measured in this run on this GPU (c8r_probe_peaks); "
+                       "of measured",
+        "traffic_source": "profiles/windowed_kernel_tiled_c1_1m.md (ncu, 1e6-track capture, "
+                          "scaled per track)",
+        "hbm": {"bytes_per_launch": traffic.get("zhs"),
+                "achieved_gbs": (traffic.get("zhs") or 0) / (zhs_ms * 1e-3) / 1e9 if zhs_ms else None,
+                "peak_gbs": hbm_peak_gbs()},
+        "secondary": dict(roof(coreas_flops, coreas_ms, "coreas"),
+                          kernel="windowed_kernel<fixed,float,CoREAS>"),
+        "atomics": {"shared_per_s_peak": peaks["shared_atomics_per_s"],
+                    "global_per_s_peak": peaks["global_atomics_per_s"],
+                    "samples_per_s": (per["coreas_contributions"] + per["zhs_contributions"]) /
+                                     ((zhs_ms + coreas_ms) * 1e-3) if zhs_ms + coreas_ms else None},
+    })
 
     e2e = None
     if not args.no_e2e:
@@ -305,7 +337,7 @@ def run_ours(args):
                    "kernel": args.kernel, "pairs_per_step": pairs_per_step,
                    "l2": "inputs larger than L2 (7.5 GB records, 1.1 GB kinematics)"},
         "e2e": e2e, "roofline": roofline, "cpu_baseline": baseline,
-        "clocks": clocks, "gpu_launches": 2 * args.steps,
+        "clocks": clocks, "gpu_launches": 3 * args.steps,
         "counters": {k: counters[k] for k in ("valid_tracks", "coreas_contributions",
                                               "zhs_contributions", "zhs_subtracks",
                                               "fixed_point_overflows")},

@@ -195,6 +195,8 @@ class Statistics(C.Structure):
         ("observer_tile_size", C.c_uint32),
         ("kernel_time_ms", C.c_double),
         ("timed_launches", C.c_uint64),
+        ("coreas_kernel_time_ms", C.c_double),
+        ("zhs_kernel_time_ms", C.c_double),
         ("counters", Counters),
     ]
 

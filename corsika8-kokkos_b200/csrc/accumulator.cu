@@ -360,19 +360,26 @@ class Accumulator {
     if (timing_) {
       end = timing_event();
       check(cudaEventRecord(end, stream_), "event");
-      pending_.push_back({begin, end});
+      pending_.push_back({{begin, end}, -1});
     }
     downloaded_ = false;
   }
 
   // Sums the projection-kernel time of completed launches (blocks on them).
   void resolve_timing() {
-    for (auto const& p : pending_) {
+    for (auto const& entry : pending_) {
+      auto const& p = entry.first;
       check(cudaEventSynchronize(p.second), "event");
       float ms = 0.f;
       check(cudaEventElapsedTime(&ms, p.first, p.second), "event time");
-      stats_.kernel_time_ms += ms;
-      ++stats_.timed_launches;
+      if (entry.second == 0)
+        stats_.coreas_kernel_time_ms += ms;
+      else if (entry.second == 1)
+        stats_.zhs_kernel_time_ms += ms;
+      else {
+        stats_.kernel_time_ms += ms;
+        ++stats_.timed_launches;
+      }
       free_events_.push_back(p.first);
       free_events_.push_back(p.second);
     }
@@ -720,8 +727,18 @@ class Accumulator {
       uint64_t ctas = static_cast<uint64_t>(per_sm) * sms_;
       if (ctas > plan.total_items) ctas = plan.total_items;
       check(cudaMemsetAsync(next_item_.ptr, 0, sizeof(unsigned), stream_), "memset");
+      cudaEvent_t b = nullptr, e = nullptr;
+      if (timing_) {
+        b = timing_event();
+        check(cudaEventRecord(b, stream_), "event");
+      }
       check(launch_windowed(plan, fixed_, precision_, static_cast<int>(ctas), threads_, stream_),
             "windowed launch");
+      if (timing_) {
+        e = timing_event();
+        check(cudaEventRecord(e, stream_), "event");
+        pending_.push_back({{b, e}, algorithm});
+      }
       stats_.projection_tiles += plan.total_items;
     }
     uint64_t const pairs_c = count * ev.observer_count[0];
@@ -781,7 +798,9 @@ class Accumulator {
   cudaEvent_t consumed_[2] = {nullptr, nullptr};
   PinnedBuffer<c8r_lepton_transport_record> host_[2];
   cudaEvent_t host_ready_[2] = {nullptr, nullptr};
-  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending_;
+  // (begin, end) event pairs; tag -1 = a whole accumulate's projection,
+  // 0 / 1 = the windowed CoREAS / ZHS launch inside it
+  std::vector<std::pair<std::pair<cudaEvent_t, cudaEvent_t>, int>> pending_;
   std::vector<cudaEvent_t> free_events_, all_events_;
   int host_index_ = 0;
   std::size_t host_count_ = 0;

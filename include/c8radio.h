@@ -192,7 +192,9 @@ typedef struct c8r_statistics {
   uint32_t track_tile_size;
   uint32_t observer_tile_size;
   double kernel_time_ms;      /* CUDA-event time of projection kernels (timing on) */
-  uint64_t timed_launches;    /* projection launches included in kernel_time_ms */
+  uint64_t timed_launches;    /* accumulate calls included in kernel_time_ms */
+  double coreas_kernel_time_ms; /* windowed CoREAS launches alone (timing on) */
+  double zhs_kernel_time_ms;    /* windowed ZHS launches alone (timing on) */
   c8r_counters counters;      /* last downloaded device counters */
 } c8r_statistics;
 
