@@ -350,3 +350,68 @@ class RadioAccumulator:
 
     def set_kernel_timing(self, enabled: bool) -> None:
         self._check(self._lib.c8r_set_kernel_timing(self._h, int(enabled)))
+
+    # B200 extensions: staging for batched projection -----------------------
+    def stage_lepton_tracks(self, device_pointer: int, count: int,
+                            extent: Optional[int] = None) -> None:
+        """Ingests device records without projecting them (see RadioBatch)."""
+        self._check(self._lib.c8r_stage_device(
+            self._h, C.c_void_p(device_pointer), count, count if extent is None else extent))
+
+    def project_staged(self) -> None:
+        self._check(self._lib.c8r_project_staged(self._h))
+
+    def set_tuning(self, tuning: TuningParameters) -> None:
+        t = tuning.to_c()
+        self._check(self._lib.c8r_set_tuning(self._h, C.byref(t)))
+
+
+class RadioBatch:
+    """Projects the staged tracks of several accumulators (one shower each, same
+    stream, precision and trace mode) with one persistent launch per algorithm,
+    optionally replayed from a captured CUDA graph (graph=True needs a
+    non-default stream)."""
+
+    def __init__(self, stream: Optional[int] = None):
+        self._lib = library()
+        handle = C.c_void_p()
+        _raise(self._lib.c8r_batch_create(C.c_void_p(stream or 0), C.byref(handle)),
+               self._lib.c8r_last_global_error())
+        self._h = handle
+
+    def _check(self, status: int) -> None:
+        if status != abi.C8R_OK:
+            _raise(status, self._lib.c8r_batch_last_error(self._h))
+
+    @staticmethod
+    def _handles(events):
+        return (C.c_void_p * len(events))(*[e._h.value for e in events])
+
+    def project(self, events, graph: bool = False, keep_staged: bool = False) -> None:
+        flags = (abi.BATCH_GRAPH if graph else 0) | (abi.BATCH_KEEP_STAGED if keep_staged else 0)
+        self._check(self._lib.c8r_batch_project(self._h, self._handles(events), len(events), flags))
+
+    def autotune(self, events, repetitions: int = 2):
+        best = abi.Tuning()
+        ms = C.c_double()
+        self._check(self._lib.c8r_batch_autotune(self._h, self._handles(events), len(events),
+                                                 repetitions, C.byref(best), C.byref(ms)))
+        return TuningParameters(best.batch_size, best.chunk_size, best.team_size,
+                                best.track_tile_size, best.observer_tile_size,
+                                best.device_queues), ms.value
+
+    def graph_captures(self) -> int:
+        out = C.c_ulonglong()
+        self._check(self._lib.c8r_batch_graph_captures(self._h, C.byref(out)))
+        return out.value
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.c8r_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -71,6 +71,8 @@ PRECISION_MIXED = 1
 KERNEL_AUTO = 0
 KERNEL_DIRECT = 1
 KERNEL_WINDOWED = 2
+BATCH_GRAPH = 1
+BATCH_KEEP_STAGED = 2
 
 
 class ObserverSnapshot(C.Structure):
@@ -232,6 +234,16 @@ PROTOTYPES = {
     "c8r_synchronize": (C.c_int, [C.c_void_p]),
     "c8r_set_kernel_timing": (C.c_int, [C.c_void_p, C.c_int]),
     "c8r_probe_peaks": (C.c_int, [C.POINTER(Peaks)]),
+    "c8r_stage_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_size_t]),
+    "c8r_project_staged": (C.c_int, [C.c_void_p]),
+    "c8r_set_tuning": (C.c_int, [C.c_void_p, C.POINTER(Tuning)]),
+    "c8r_batch_create": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "c8r_batch_destroy": (None, [C.c_void_p]),
+    "c8r_batch_last_error": (C.c_char_p, [C.c_void_p]),
+    "c8r_batch_project": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.c_size_t, C.c_int]),
+    "c8r_batch_autotune": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.c_size_t, C.c_int,
+                                     C.POINTER(Tuning), C.POINTER(C.c_double)]),
+    "c8r_batch_graph_captures": (C.c_int, [C.c_void_p, C.POINTER(C.c_ulonglong)]),
 }
 
 

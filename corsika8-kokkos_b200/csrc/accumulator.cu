@@ -9,7 +9,9 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <cstring>
+#include <map>
 #include <limits>
 #include <mutex>
 #include <new>
@@ -59,6 +61,10 @@ struct DeviceBuffer {
     count = 0;
   }
   std::size_t bytes() const { return count * sizeof(T); }
+  void swap(DeviceBuffer& other) noexcept {
+    std::swap(ptr, other.ptr);
+    std::swap(count, other.count);
+  }
 };
 
 template <class T>
@@ -237,6 +243,7 @@ class Accumulator {
         check(cudaMemsetAsync(float_traces_[a].ptr, 0, float_traces_[a].bytes(), stream_), "memset");
     }
     check(cudaMemsetAsync(counters_.ptr, 0, sizeof(DeviceCounters), stream_), "memset");
+    clear_staged();
     check(cudaStreamSynchronize(stream_), "reset fence");
     resolve_timing();
     stats_ = c8r_statistics{};
@@ -331,21 +338,42 @@ class Accumulator {
     ++stats_.host_track_batches;
   }
 
-  // RadioAccumulator::accumulateLeptonTracks, RadioAccumulator.inl:292-357.
+  // RadioAccumulator::accumulateLeptonTracks, RadioAccumulator.inl:292-357:
+  // ingest the records and project them (with any tracks staged before).
   void accumulate_device(c8r_lepton_transport_record const* records, std::size_t count,
                          std::size_t extent) {
+    if (!enabled() || count == 0) return;
+    stage_device(records, count, extent);
+    project_staged(true);
+  }
+
+  // B200 extension: ingest device records into the kinematics workspace,
+  // after the tracks already staged, without projecting them yet.
+  void stage_device(c8r_lepton_transport_record const* records, std::size_t count,
+                    std::size_t extent) {
     if (!enabled() || count == 0) return;
     if (sealed_) throw std::logic_error("radio endpoint already committed; reset before new tracks");
     if (count > extent) throw std::out_of_range("radio track count exceeds input view");
     if (records == nullptr) throw std::invalid_argument("null device radio track input");
-    ensure_capacity(count);
-    check(cudaMemsetAsync(slot_.ptr, 0, sizeof(unsigned long long), stream_), "memset");
+    if (staged_ > std::numeric_limits<std::size_t>::max() - count)
+      throw std::length_error("radio staged track count overflow");
+    ensure_capacity(staged_ + count);
+    if (staged_ == 0) check(cudaMemsetAsync(slot_.ptr, 0, sizeof(unsigned long long), stream_), "memset");
     check(launch_ingest(records, count, tracks_.ptr, capacity_, slot_.ptr, counters_.ptr,
                         diagnostics_, stream_),
           "ingest launch");
+    staged_ += count;
     ++stats_.track_precompute_batches;
     stats_.track_precomputed_records += count;
     stats_.maximum_track_batch = std::max<uint64_t>(stats_.maximum_track_batch, count);
+    downloaded_ = false;
+  }
+
+  // Projects the staged tracks of this accumulator alone; consume drops them.
+  void project_staged(bool consume) {
+    if (!enabled() || staged_ == 0) return;
+    if (sealed_) throw std::logic_error("radio endpoint already committed; reset before new tracks");
+    std::size_t const count = staged_;
     cudaEvent_t begin = nullptr, end = nullptr;
     if (timing_) {
       begin = timing_event();
@@ -362,7 +390,48 @@ class Accumulator {
       check(cudaEventRecord(end, stream_), "event");
       pending_.push_back({{begin, end}, -1});
     }
+    if (consume) clear_staged();
     downloaded_ = false;
+  }
+
+  void clear_staged() {
+    if (staged_ == 0) return;
+    check(cudaMemsetAsync(slot_.ptr, 0, sizeof(unsigned long long), stream_), "memset");
+    staged_ = 0;
+  }
+
+  // Batched projection support (Batch below).
+  std::size_t staged() const { return staged_; }
+  cudaStream_t stream() const { return stream_; }
+  bool sealed() const { return sealed_; }
+  void note_batch_projection(std::size_t count, uint64_t items) {
+    EventPlan const ev = make_event(count);
+    uint64_t const pairs_c = count * ev.observer_count[0], pairs_z = count * ev.observer_count[1];
+    stats_.track_observer_pairs += pairs_c + pairs_z;
+    if (fuse_) stats_.fused_track_observer_pairs += pairs_c;
+    stats_.projection_tiles += items;
+    downloaded_ = false;
+  }
+  void set_tuning(c8r_tuning const& t) {
+    if (t.team_size > static_cast<uint64_t>(kWindowThreads) || (t.team_size != 0 && t.team_size % 32 != 0))
+      throw std::invalid_argument("radio tuning is invalid");
+    threads_ = t.team_size ? static_cast<int>(t.team_size) : 512;
+    tuning_.team_size = t.team_size;
+    tuning_.track_tile_size = t.track_tile_size;
+    stats_.track_tile_size = static_cast<uint32_t>(t.track_tile_size);
+  }
+  // Zeroes traces and projection counters, keeping staged tracks (autotuning).
+  void zero_traces() {
+    if (!enabled()) return;
+    for (int a = 0; a < 2; ++a) {
+      if (fixed_traces_[a].ptr)
+        check(cudaMemsetAsync(fixed_traces_[a].ptr, 0, fixed_traces_[a].bytes(), stream_), "memset");
+      if (float_traces_[a].ptr)
+        check(cudaMemsetAsync(float_traces_[a].ptr, 0, float_traces_[a].bytes(), stream_), "memset");
+    }
+    check(cudaMemsetAsync(counters_.ptr, 0, offsetof(DeviceCounters, valid_tracks), stream_), "memset");
+    check(cudaMemsetAsync(&counters_.ptr->fixed_point_overflows, 0, sizeof(unsigned long long), stream_),
+          "memset");
   }
 
   // Sums the projection-kernel time of completed launches (blocks on them).
@@ -394,6 +463,7 @@ class Accumulator {
     }
     if (downloaded_ || sealed_) throw std::logic_error("radio waveforms downloaded twice");
     flush();
+    project_staged(true);
     DeviceCounters host{};
     fetch_counters(host);
     if (host.fixed_point_overflows != 0)
@@ -429,6 +499,7 @@ class Accumulator {
     if (!enabled() || !fixed_ || downloaded_ || sealed_)
       throw std::logic_error("fixed radio snapshot unavailable/already committed");
     flush();
+    project_staged(true);
     sealed_ = true;
     DeviceCounters host{};
     fetch_counters(host);
@@ -653,8 +724,15 @@ class Accumulator {
     if (capacity_ > std::numeric_limits<std::size_t>::max() / 2)
       throw std::length_error("radio track capacity overflow");
     std::size_t const grown = capacity_ == 0 ? count : std::max(count, 2 * capacity_);
+    DeviceBuffer<double> fresh;
+    fresh.allocate(checked_mul(grown, kTrackDoubles));
+    if (staged_ != 0)  // keep the tracks staged so far
+      check(cudaMemcpyAsync(fresh.ptr, tracks_.ptr, staged_ * kTrackDoubles * sizeof(double),
+                            cudaMemcpyDeviceToDevice, stream_),
+            "staged track copy");
+    // earlier projections may still read the old workspace
     if (capacity_ != 0) check(cudaStreamSynchronize(stream_), "grow fence");
-    tracks_.allocate(checked_mul(grown, kTrackDoubles));
+    tracks_.swap(fresh);
     capacity_ = grown;
     stats_.track_workspace_bytes = tracks_.bytes();
     stats_.device_bytes = device_bytes();
@@ -663,7 +741,8 @@ class Accumulator {
   std::size_t chunk_hint() const { return tuning_.track_tile_size; }
 
   EventPlan make_event(std::size_t count) const {
-    EventPlan ev{};
+    EventPlan ev;
+    std::memset(&ev, 0, sizeof ev);
     ev.tracks = tracks_.ptr;
     ev.stride = capacity_;
     ev.valid_tracks = slot_.ptr;
@@ -792,6 +871,7 @@ class Accumulator {
   DeviceBuffer<unsigned> next_item_;
   DeviceBuffer<double> tracks_;
   std::size_t capacity_ = 0;
+  std::size_t staged_ = 0;  // records ingested since the last projection (upper bound of tracks)
   DeviceBuffer<c8r_lepton_transport_record> staging_, staging2_;
   cudaStream_t copy_stream_ = nullptr;
   cudaEvent_t copy_done_[2] = {nullptr, nullptr};
@@ -808,11 +888,207 @@ class Accumulator {
   c8r_statistics stats_{};
 };
 
+
+// Batched projection: the staged tracks of many
+// accumulators projected by one persistent launch per algorithm (up to
+// kMaxEventsPerLaunch events a launch), optionally replayed from a CUDA graph
+// captured per distinct launch plan.
+class Batch {
+ public:
+  explicit Batch(cudaStream_t stream) : stream_(stream) {
+    next_item_.allocate(1);
+  }
+  ~Batch() {
+    if (stream_) cudaStreamSynchronize(stream_);
+    for (auto& g : graphs_) {
+      cudaGraphExecDestroy(g.second.exec);
+      cudaGraphDestroy(g.second.graph);
+    }
+  }
+
+  void project(Accumulator* const* events, std::size_t n, int flags) {
+    auto plans = plan(events, n);
+    if (plans.launches.empty()) return;
+    bool const graph = (flags & C8R_BATCH_GRAPH) != 0;
+    if (graph) {
+      if (stream_ == nullptr)
+        throw std::invalid_argument("graph replay needs a non-default CUDA stream");
+      std::string key(reinterpret_cast<char const*>(plans.launches.data()),
+                      plans.launches.size() * sizeof(Launch));
+      auto it = graphs_.find(key);
+      if (it == graphs_.end()) {
+        Graph g{};
+        check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "graph capture");
+        try {
+          enqueue(plans);
+        } catch (...) {
+          cudaGraph_t discard = nullptr;
+          cudaStreamEndCapture(stream_, &discard);
+          if (discard) cudaGraphDestroy(discard);
+          throw;
+        }
+        check(cudaStreamEndCapture(stream_, &g.graph), "graph capture");
+        check(cudaGraphInstantiate(&g.exec, g.graph, 0), "graph instantiate");
+        it = graphs_.emplace(std::move(key), g).first;
+        ++captures_;
+      }
+      check(cudaGraphLaunch(it->second.exec, stream_), "graph launch");
+    } else {
+      enqueue(plans);
+    }
+    for (std::size_t i = 0; i < n; ++i) {
+      if (!events[i]->enabled() || events[i]->staged() == 0) continue;
+      events[i]->note_batch_projection(events[i]->staged(), plans.items[i]);
+      if (!(flags & C8R_BATCH_KEEP_STAGED)) events[i]->clear_staged();
+    }
+  }
+
+  // Sweeps block size x chunk size (tracks per work item) on the staged
+  // events, keeps the fastest, and zeroes the traces it wrote.
+  c8r_tuning autotune(Accumulator* const* events, std::size_t n, int repetitions, double& best_ms) {
+    static constexpr uint64_t kTeams[] = {256, 384, 512};
+    static constexpr uint64_t kChunks[] = {0, 32768, 131072, 524288};
+    c8r_tuning best{};
+    best_ms = -1.;
+    cudaEvent_t a = nullptr, b = nullptr;
+    check(cudaEventCreate(&a), "event");
+    check(cudaEventCreate(&b), "event");
+    for (uint64_t team : kTeams) {
+      for (uint64_t chunk : kChunks) {
+        c8r_tuning t{};
+        t.team_size = team;
+        t.track_tile_size = chunk;
+        for (std::size_t i = 0; i < n; ++i) events[i]->set_tuning(t);
+        project(events, n, C8R_BATCH_KEEP_STAGED);  // warm
+        check(cudaEventRecord(a, stream_), "event");
+        for (int r = 0; r < repetitions; ++r) project(events, n, C8R_BATCH_KEEP_STAGED);
+        check(cudaEventRecord(b, stream_), "event");
+        check(cudaEventSynchronize(b), "event");
+        float ms = 0.f;
+        check(cudaEventElapsedTime(&ms, a, b), "event time");
+        double const per = ms / repetitions;
+        if (best_ms < 0. || per < best_ms) {
+          best_ms = per;
+          best = t;
+        }
+      }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    for (std::size_t i = 0; i < n; ++i) {
+      events[i]->set_tuning(best);
+      events[i]->zero_traces();
+    }
+    return best;
+  }
+
+  uint64_t captures() const { return captures_; }
+
+ private:
+  struct Launch {
+    WorkPlan plan;
+    int ctas;
+    int threads;
+  };
+  struct Plans {
+    std::vector<Launch> launches;
+    std::vector<uint64_t> items;  // work items per event
+    bool fixed = true;
+    Precision precision = Precision::kFP64;
+  };
+  struct Graph {
+    cudaGraph_t graph;
+    cudaGraphExec_t exec;
+  };
+
+  Plans plan(Accumulator* const* events, std::size_t n) {
+    Plans out;
+    out.items.assign(n, 0);
+    std::vector<std::pair<std::size_t, EventPlan>> active;
+    bool fixed = true;
+    Precision precision = Precision::kFP64;
+    int threads = 0;
+    uint32_t window = 1;
+    for (std::size_t i = 0; i < n; ++i) {
+      Accumulator* e = events[i];
+      if (e == nullptr) throw std::invalid_argument("null radio accumulator in batch");
+      if (!e->enabled() || e->staged() == 0) continue;
+      if (e->sealed()) throw std::logic_error("radio endpoint already committed; reset before new tracks");
+      if (e->stream() != stream_) throw std::invalid_argument("batched accumulators must share the batch stream");
+      EventPlan ev = e->event_plan(e->staged());
+      if (active.empty()) {
+        fixed = e->fixed();
+        precision = e->precision();
+        threads = e->threads();
+      } else if (e->fixed() != fixed || e->precision() != precision) {
+        throw std::invalid_argument("batched accumulators must share precision and trace mode");
+      }
+      window = std::max(window, ev.window);
+      active.push_back({i, ev});
+    }
+    if (active.empty()) return out;
+    out.fixed = fixed;
+    out.precision = precision;
+    int device = 0, sms = 0;
+    check(cudaGetDevice(&device), "device");
+    check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "SM count");
+    int const per_sm = windowed_ctas_per_sm(static_cast<int>(window), threads, fixed, precision);
+    if (per_sm <= 0) throw cuda_error("windowed radio kernel does not fit on this device");
+    for (int algorithm = 0; algorithm < 2; ++algorithm) {
+      for (std::size_t first = 0; first < active.size();) {
+        Launch l;
+        std::memset(&l, 0, sizeof l);  // zero padding: the launch bytes key the graph cache
+        l.plan.algorithm = algorithm;
+        l.plan.window = window;
+        l.plan.next_item = next_item_.ptr;
+        l.threads = threads;
+        uint64_t items = 0;
+        std::size_t j = first;
+        for (; j < active.size() && l.plan.event_count < static_cast<uint32_t>(kMaxEventsPerLaunch); ++j) {
+          EventPlan ev = active[j].second;
+          if (ev.observer_count[algorithm] == 0) continue;
+          ev.first_item = items;
+          uint64_t const event_items = static_cast<uint64_t>(ev.chunks) * ev.observer_count[algorithm];
+          items += event_items;
+          out.items[active[j].first] += event_items;
+          l.plan.events[l.plan.event_count++] = ev;
+        }
+        first = j;
+        if (l.plan.event_count == 0) continue;
+        l.plan.total_items = items;
+        uint64_t ctas = static_cast<uint64_t>(per_sm) * sms;
+        if (ctas > items) ctas = items;
+        l.ctas = static_cast<int>(ctas);
+        out.launches.push_back(l);
+      }
+    }
+    return out;
+  }
+
+  void enqueue(Plans const& plans) {
+    for (auto const& l : plans.launches) {
+      check(cudaMemsetAsync(next_item_.ptr, 0, sizeof(unsigned), stream_), "memset");
+      check(launch_windowed(l.plan, plans.fixed, plans.precision, l.ctas, l.threads, stream_),
+            "batched windowed launch");
+    }
+  }
+
+  cudaStream_t stream_ = nullptr;
+  DeviceBuffer<unsigned> next_item_;
+  std::map<std::string, Graph> graphs_;
+  uint64_t captures_ = 0;
+};
+
 }  // namespace c8r
 
 // ============================================================== C boundary
 struct c8r_accumulator {
   c8r::Accumulator* impl = nullptr;
+  std::string error;
+};
+
+struct c8r_batch {
+  c8r::Batch* impl = nullptr;
   std::string error;
 };
 
@@ -1004,6 +1280,84 @@ int c8r_projected_track_capacity(const c8r_accumulator* handle, size_t count,
 int c8r_set_kernel_timing(c8r_accumulator* handle, int enabled) {
   if (int s = with_handle(handle, nullptr, true)) return s;
   handle->impl->set_timing(enabled != 0);
+  return C8R_OK;
+}
+
+int c8r_stage_device(c8r_accumulator* handle, const c8r_lepton_transport_record* records,
+                     size_t count, size_t extent) {
+  if (int s = with_handle(handle, nullptr, true)) return s;
+  return guarded(&handle->error, [&] { handle->impl->stage_device(records, count, extent); });
+}
+
+int c8r_project_staged(c8r_accumulator* handle) {
+  if (int s = with_handle(handle, nullptr, true)) return s;
+  return guarded(&handle->error, [&] { handle->impl->project_staged(true); });
+}
+
+int c8r_set_tuning(c8r_accumulator* handle, const c8r_tuning* tuning) {
+  if (int s = with_handle(handle, nullptr, true)) return s;
+  if (!tuning) return C8R_INVALID_ARGUMENT;
+  return guarded(&handle->error, [&] { handle->impl->set_tuning(*tuning); });
+}
+
+int c8r_batch_create(void* stream, c8r_batch** batch) {
+  return guarded(&g_last_error, [&] {
+    if (!batch) throw std::invalid_argument("null argument");
+    auto* b = new c8r_batch;
+    try {
+      b->impl = new c8r::Batch(static_cast<cudaStream_t>(stream));
+    } catch (...) {
+      delete b;
+      throw;
+    }
+    *batch = b;
+  });
+}
+
+void c8r_batch_destroy(c8r_batch* batch) {
+  if (!batch) return;
+  delete batch->impl;
+  delete batch;
+}
+
+const char* c8r_batch_last_error(const c8r_batch* batch) {
+  return batch ? batch->error.c_str() : g_last_error.c_str();
+}
+
+static std::vector<c8r::Accumulator*> unwrap(c8r_accumulator* const* events, size_t count) {
+  if (count != 0 && events == nullptr) throw std::invalid_argument("null radio accumulator list");
+  std::vector<c8r::Accumulator*> out(count);
+  for (size_t i = 0; i < count; ++i) {
+    if (events[i] == nullptr || events[i]->impl == nullptr)
+      throw std::invalid_argument("null radio accumulator in batch");
+    out[i] = events[i]->impl;
+  }
+  return out;
+}
+
+int c8r_batch_project(c8r_batch* batch, c8r_accumulator* const* events, size_t count, int flags) {
+  if (!batch || !batch->impl) return C8R_INVALID_ARGUMENT;
+  return guarded(&batch->error, [&] {
+    auto list = unwrap(events, count);
+    batch->impl->project(list.data(), list.size(), flags);
+  });
+}
+
+int c8r_batch_autotune(c8r_batch* batch, c8r_accumulator* const* events, size_t count,
+                       int repetitions, c8r_tuning* best, double* best_ms) {
+  if (!batch || !batch->impl) return C8R_INVALID_ARGUMENT;
+  return guarded(&batch->error, [&] {
+    auto list = unwrap(events, count);
+    double ms = 0.;
+    c8r_tuning const t = batch->impl->autotune(list.data(), list.size(), repetitions > 0 ? repetitions : 1, ms);
+    if (best) *best = t;
+    if (best_ms) *best_ms = ms;
+  });
+}
+
+int c8r_batch_graph_captures(const c8r_batch* batch, unsigned long long* captures) {
+  if (!batch || !batch->impl || !captures) return C8R_INVALID_ARGUMENT;
+  *captures = batch->impl->captures();
   return C8R_OK;
 }
 

@@ -306,3 +306,47 @@ def make_config(workload: dict, precision: int = 0, kernel: int = 0, determinist
                        coreas_observers=obs if coreas else np.zeros(0, OBSERVER),
                        zhs_observers=obs if zhs else np.zeros(0, OBSERVER),
                        precision=precision, kernel=kernel, **extra)
+
+
+# ---------------------------------------------------------------- many events
+@dataclass
+class EventSpec:
+    """One shower of a batched or served workload."""
+
+    seed: int
+    segments: int
+    antennas: int
+    zenith_deg: float
+    xmax: float
+    bins: int = 4096
+
+
+def batched_event_specs(events: int = 64, seed: int = 2024, min_segments: int = 100_000,
+                        max_segments: int = 20_000_000, min_antennas: int = 16,
+                        max_antennas: int = 300, bins: int = 4096) -> list:
+    """Events of the batched workload: segment counts log-uniform in
+    [min, max], antenna stars of 16..300 antennas (8 arms), zenith uniform in
+    0..60 deg, Xmax uniform in 550..850 g/cm^2, all from one seed."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for k in range(events):
+        segments = int(np.exp(rng.uniform(math.log(min_segments), math.log(max_segments))))
+        antennas = int(rng.integers(min_antennas, max_antennas + 1))
+        out.append(EventSpec(seed=seed * 7919 + k, segments=segments, antennas=antennas,
+                             zenith_deg=float(rng.uniform(0.0, 60.0)),
+                             xmax=float(rng.uniform(550.0, 850.0)), bins=bins))
+    return out
+
+
+def event_workload(spec: EventSpec, ground_z_m: float = 1400.0):
+    """(workload dict, generator kwargs) of one event: a star of 8 arms with
+    ceil(antennas/8) radii spread over 25..500 m (trimmed to `antennas`),
+    4096-sample traces at 0.1 ns."""
+    arms = 8
+    radii = list(np.linspace(25.0, 500.0, max(1, -(-spec.antennas // arms))))
+    observers = star_antennas(arms, radii, ground_z_m, spec.bins, 1e10,
+                              zenith_deg=spec.zenith_deg)[: spec.antennas]
+    model = AtmosphereModel()
+    table = flat_atmosphere_table(model, ground_z_m, 30000.0, 1.0)
+    gen = dict(zenith_deg=spec.zenith_deg, xmax=spec.xmax, ground_z_m=ground_z_m, model=model)
+    return dict(observers=observers, table=table, homogeneous=0.0), gen

@@ -277,6 +277,41 @@ int c8r_probe_peaks(c8r_peaks* peaks);
 /* Blocks until all work queued on the accumulator's stream has completed. */
 int c8r_synchronize(c8r_accumulator* handle);
 
+/* ---- B200 extensions: staging and batched projection ---------------------
+ * No reference counterpart: the reference projects every accumulateLeptonTracks
+ * batch on its own (RadioAccumulator.inl:292-357).  Here ingest and projection
+ * can be separated so that many events share one persistent launch. */
+
+/* Ingests device records into the accumulator's kinematics workspace after
+ * the tracks already staged, without projecting them (same checks as
+ * c8r_accumulate_device).  download/download_fixed project staged tracks. */
+int c8r_stage_device(c8r_accumulator* handle, const c8r_lepton_transport_record* records,
+                     size_t count, size_t extent);
+/* Projects and drops this accumulator's staged tracks. */
+int c8r_project_staged(c8r_accumulator* handle);
+/* Changes team_size (threads per windowed CTA) and track_tile_size (tracks per
+ * work item, 0 = automatic) of an accumulator. */
+int c8r_set_tuning(c8r_accumulator* handle, const c8r_tuning* tuning);
+
+typedef struct c8r_batch c8r_batch;
+enum {
+  C8R_BATCH_GRAPH = 1,       /* replay a CUDA graph captured per distinct launch plan */
+  C8R_BATCH_KEEP_STAGED = 2  /* keep the staged tracks after projecting them */
+};
+/* A batch projects the staged tracks of several accumulators (one shower each,
+ * same stream, precision and trace mode) with one persistent launch per
+ * algorithm for up to 64 events; graph replay needs a non-default stream. */
+int c8r_batch_create(void* stream, c8r_batch** batch);
+void c8r_batch_destroy(c8r_batch* batch);
+const char* c8r_batch_last_error(const c8r_batch* batch);
+int c8r_batch_project(c8r_batch* batch, c8r_accumulator* const* events, size_t count, int flags);
+/* Sweeps team size {256,384,512} x tracks per item {auto,32768,131072,524288}
+ * on the staged events (repetitions timed runs each), applies the fastest to
+ * every event, zeroes the traces the sweep wrote and returns it. */
+int c8r_batch_autotune(c8r_batch* batch, c8r_accumulator* const* events, size_t count,
+                       int repetitions, c8r_tuning* best, double* best_ms);
+int c8r_batch_graph_captures(const c8r_batch* batch, unsigned long long* captures);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif
