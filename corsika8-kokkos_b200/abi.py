@@ -244,6 +244,8 @@ PROTOTYPES = {
     "c8r_batch_autotune": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.c_size_t, C.c_int,
                                      C.POINTER(Tuning), C.POINTER(C.c_double)]),
     "c8r_batch_graph_captures": (C.c_int, [C.c_void_p, C.POINTER(C.c_ulonglong)]),
+    "c8r_accumulate_device_no_alloc": (C.c_int, [C.POINTER(Config), C.c_void_p, C.c_size_t, C.c_size_t,
+                                                 C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
 }
 
 

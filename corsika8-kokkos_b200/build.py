@@ -15,7 +15,7 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 CSRC = HERE / "csrc"
 LIBRARY = HERE / "libc8radio.so"
-SOURCES = ["radio_kernels.cu", "accumulator.cu", "probes.cu", "batch.cu"]
+SOURCES = ["radio_kernels.cu", "accumulator.cu", "probes.cu", "no_alloc.cu"]
 HEADERS = ["radio_device.cuh", "radio_kernels.cuh"]
 
 NVCC_FLAGS = [

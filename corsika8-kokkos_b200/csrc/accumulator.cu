@@ -1142,6 +1142,11 @@ int with_handle(c8r_accumulator const* h, std::string* error_slot, bool need) {
 
 }  // namespace
 
+namespace c8r {
+// Error text of entry points defined in other files (c8r_last_global_error).
+void set_global_error(char const* message) { g_last_error = message; }
+}  // namespace c8r
+
 extern "C" {
 
 const char* c8r_version(void) { return "c8radio-b200 1.0 (sm_100a)"; }

@@ -312,6 +312,43 @@ int c8r_batch_autotune(c8r_batch* batch, c8r_accumulator* const* events, size_t 
                        int repetitions, c8r_tuning* best, double* best_ms);
 int c8r_batch_graph_captures(const c8r_batch* batch, unsigned long long* captures);
 
+/* ---- Accumulate without allocating device memory ---------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory when they project tracks: a transport code that has given all of HBM
+ * to its own pool allocator (a Kokkos memory pool, a particle stack sized to
+ * the card), or one that drives several streams and cannot accept the device
+ * synchronisation of cudaMalloc/cudaFree.
+ *
+ * Ingests `count` device records (count <= extent) and adds their CoREAS
+ * field and ZHS potential into CALLER-OWNED device traces, with the
+ * accumulator's trace layout and units: rows [X | Y | Z] of the algorithm's
+ * total bins, observers in config order; long long fixed-point values when
+ * config->deterministic (as c8r_download_fixed returns them), else double.
+ * `counters` is a device c8r_counters added into, or NULL.  The caller zeroes
+ * traces and counters before its first call; later calls add to them, as
+ * c8r_accumulate_device does.  config->kernel is ignored (always the windowed
+ * projection).  Host arrays of the config are read before the call returns;
+ * the work itself is queued on `stream`.
+ *
+ * Scratch: one static device array of C8R_NO_ALLOC_SCRATCH_BYTES per GPU that
+ * loads this library's module, held until the process exits.  The call calls
+ * no cudaMalloc, cudaFree or other allocating routine.  Its first call on a
+ * device sets up that device (looks up the array's address, loading the
+ * module there if needed): make that first call before any stream capture.
+ * All calls on a device share the array, so calls that overlap on the GPU
+ * race: keep them ordered on one stream.  Records are processed in chunks
+ * that fit the array, so `count` has no limit; more than
+ * C8R_NO_ALLOC_MAX_OBSERVERS observers (CoREAS + ZHS) or a refractivity table
+ * of more than C8R_NO_ALLOC_MAX_TABLE_ENTRIES entries is rejected with
+ * C8R_LENGTH_ERROR before any device work. */
+#define C8R_NO_ALLOC_SCRATCH_BYTES (32u << 20)
+#define C8R_NO_ALLOC_MAX_OBSERVERS 2048u
+#define C8R_NO_ALLOC_MAX_TABLE_ENTRIES 131072u
+int c8r_accumulate_device_no_alloc(const c8r_config* config,
+                                   const c8r_lepton_transport_record* records, size_t count,
+                                   size_t extent, void* coreas_traces, void* zhs_traces,
+                                   c8r_counters* counters, void* stream);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif
