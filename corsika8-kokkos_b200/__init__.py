@@ -63,6 +63,10 @@ class AllocationError(RadioError, MemoryError):
     """device or pinned allocation failure"""
 
 
+class ServerTimeout(RadioError, TimeoutError):
+    """server: not admitted / not complete within the timeout"""
+
+
 _STATUS = {
     abi.C8R_INVALID_ARGUMENT: InvalidArgument,
     abi.C8R_LOGIC_ERROR: LogicError,
@@ -72,6 +76,7 @@ _STATUS = {
     abi.C8R_OVERFLOW_ERROR: OverflowErrorRadio,
     abi.C8R_CUDA_ERROR: CudaError,
     abi.C8R_BAD_ALLOC: AllocationError,
+    abi.C8R_TIMEOUT: ServerTimeout,
 }
 
 _lib: Optional[C.CDLL] = None
@@ -415,3 +420,93 @@ class RadioBatch:
             self.close()
         except Exception:
             pass
+
+
+class RadioServer:
+    """Many showers in flight on one GPU (c8r_server_*): events are admitted
+    against an HBM budget reserved at creation, their tracks are added as
+    device records, and a scheduler thread projects every ready event in
+    rounds of one persistent launch per algorithm.  Thread-safe."""
+
+    def __init__(self, budget_bytes: int, block_tracks: int = 0, chunk_tracks: int = 0,
+                 round_pairs: int = 0, team_size: int = 0):
+        self._lib = library()
+        opts = abi.ServerOptions(budget_bytes, block_tracks, chunk_tracks, round_pairs, team_size)
+        handle = C.c_void_p()
+        status = self._lib.c8r_server_create(C.byref(opts), C.byref(handle))
+        _raise(status, self._lib.c8r_server_last_error(None))
+        self._h = handle
+        self._configs = {}
+
+    def _check(self, status: int) -> None:
+        if status != abi.C8R_OK:
+            _raise(status, self._lib.c8r_server_last_error(self._h))
+
+    def open(self, config: RadioConfig, timeout_ms: int = -1) -> int:
+        cfg, keep = config.to_c()
+        event = C.c_uint64()
+        self._check(self._lib.c8r_server_open(self._h, C.byref(cfg), timeout_ms, C.byref(event)))
+        nc = int(sum(int(b) for b in config.coreas_observers["number_of_bins"])) if config.coreas_enabled else 0
+        nz = int(sum(int(b) for b in config.zhs_observers["number_of_bins"])) if config.zhs_enabled else 0
+        self._configs[event.value] = (nc, nz)
+        return event.value
+
+    def add_device(self, event: int, device_pointer: int, count: int, stream: Optional[int] = None,
+                   extent: Optional[int] = None) -> None:
+        self._check(self._lib.c8r_server_add_device(
+            self._h, event, C.c_void_p(device_pointer), count, count if extent is None else extent,
+            C.c_void_p(stream or 0)))
+
+    def close_event(self, event: int) -> None:
+        self._check(self._lib.c8r_server_close(self._h, event))
+
+    def wait(self, event: int, timeout_ms: int = -1) -> None:
+        self._check(self._lib.c8r_server_wait(self._h, event, timeout_ms))
+
+    def fetch_fixed(self, event: int):
+        """(coreas int64 (3, bins), zhs int64 (3, bins), counters, info); releases the event."""
+        nc, nz = self._configs[event]
+        coreas = np.zeros((3, nc), np.int64)
+        zhs = np.zeros((3, nz), np.int64)
+        counters, info = abi.Counters(), abi.ServerEventInfo()
+        self._check(self._lib.c8r_server_fetch_fixed(
+            self._h, event, coreas.ctypes.data if coreas.size else None,
+            zhs.ctypes.data if zhs.size else None, C.byref(counters), C.byref(info)))
+        del self._configs[event]
+        return coreas, zhs, counters.as_dict(), info.as_dict()
+
+    def fetch(self, event: int):
+        """(RadioWaveforms decoded to V/m and V s/m, info); releases the event."""
+        nc, nz = self._configs[event]
+        coreas = np.zeros((3, nc), np.float64)
+        zhs = np.zeros((3, nz), np.float64)
+        counters, info = abi.Counters(), abi.ServerEventInfo()
+        try:
+            self._check(self._lib.c8r_server_fetch(
+                self._h, event, coreas.ctypes.data if coreas.size else None,
+                zhs.ctypes.data if zhs.size else None, C.byref(counters), C.byref(info)))
+        finally:
+            self._configs.pop(event, None)
+        return RadioWaveforms(coreas, zhs, counters.as_dict()), info.as_dict()
+
+    def stats(self) -> dict:
+        out = abi.ServerStats()
+        self._check(self._lib.c8r_server_get_stats(self._h, C.byref(out)))
+        return out.as_dict()
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.c8r_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -65,6 +65,7 @@ C8R_LENGTH_ERROR = 5
 C8R_OVERFLOW_ERROR = 6
 C8R_CUDA_ERROR = 7
 C8R_BAD_ALLOC = 8
+C8R_TIMEOUT = 9
 
 PRECISION_FP64 = 0
 PRECISION_MIXED = 1
@@ -209,6 +210,42 @@ class Peaks(C.Structure):
 
 
 # Exported symbols of libc8radio.so and their prototypes.
+class ServerOptions(C.Structure):
+    _fields_ = [
+        ("budget_bytes", C.c_uint64),
+        ("block_tracks", C.c_uint64),
+        ("chunk_tracks", C.c_uint64),
+        ("round_pairs", C.c_uint64),
+        ("team_size", C.c_uint32),
+        ("reserved_", C.c_uint32 * 7),
+    ]
+
+
+class ServerEventInfo(C.Structure):
+    _fields_ = [
+        ("records", C.c_uint64),
+        ("coreas_observers", C.c_uint64),
+        ("zhs_observers", C.c_uint64),
+        ("rounds", C.c_uint64),
+        ("open_s", C.c_double),
+        ("admitted_s", C.c_double),
+        ("closed_s", C.c_double),
+        ("completed_s", C.c_double),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class ServerStats(C.Structure):
+    _fields_ = [(name, C.c_uint64) for name in (
+        "rounds", "launches", "events_admitted", "events_completed", "blocks_allocated",
+        "arena_bytes", "arena_used_bytes", "arena_peak_bytes", "work_items")]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 PROTOTYPES = {
     "c8r_version": (C.c_char_p, []),
     "c8r_last_error": (C.c_char_p, [C.c_void_p]),
@@ -244,6 +281,19 @@ PROTOTYPES = {
     "c8r_batch_autotune": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.c_size_t, C.c_int,
                                      C.POINTER(Tuning), C.POINTER(C.c_double)]),
     "c8r_batch_graph_captures": (C.c_int, [C.c_void_p, C.POINTER(C.c_ulonglong)]),
+    "c8r_server_create": (C.c_int, [C.POINTER(ServerOptions), C.POINTER(C.c_void_p)]),
+    "c8r_server_destroy": (None, [C.c_void_p]),
+    "c8r_server_last_error": (C.c_char_p, [C.c_void_p]),
+    "c8r_server_open": (C.c_int, [C.c_void_p, C.POINTER(Config), C.c_int, C.POINTER(C.c_uint64)]),
+    "c8r_server_add_device": (C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p, C.c_size_t, C.c_size_t,
+                                        C.c_void_p]),
+    "c8r_server_close": (C.c_int, [C.c_void_p, C.c_uint64]),
+    "c8r_server_wait": (C.c_int, [C.c_void_p, C.c_uint64, C.c_int]),
+    "c8r_server_fetch_fixed": (C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p,
+                                         C.POINTER(Counters), C.POINTER(ServerEventInfo)]),
+    "c8r_server_fetch": (C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p,
+                                   C.POINTER(Counters), C.POINTER(ServerEventInfo)]),
+    "c8r_server_get_stats": (C.c_int, [C.c_void_p, C.POINTER(ServerStats)]),
     "c8r_accumulate_device_no_alloc": (C.c_int, [C.POINTER(Config), C.c_void_p, C.c_size_t, C.c_size_t,
                                                  C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
 }

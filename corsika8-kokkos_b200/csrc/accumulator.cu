@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "../../include/c8radio.h"
+#include "host_setup.hpp"
 #include "radio_kernels.cuh"
 
 namespace c8r {
@@ -618,30 +619,10 @@ class Accumulator {
     std::size_t offset = 0;
     bool const homogeneous = propagation_.homogeneous > 0.;
     for (auto const& s : snapshots_[a]) {
-      ObserverCache o{};
-      o.px = s.position_m[0];
-      o.py = s.position_m[1];
-      o.pz = s.position_m[2];
-      o.start_time = s.start_time_s;
-      o.end_time = s.start_time_s + s.duration_s;
-      o.sample_rate = s.sample_rate_hz;
-      o.resolution = 1. / s.sample_rate_hz;
-      o.wavelength = kSpeedOfLight / s.sample_rate_hz;
-      double const factor = a == 1 ? s.sample_rate_hz : 1.;
-      o.fixed_scale = deterministic_ ? kHeadroom * factor / limit_ : 1.;
-      o.fixed_scale_f = static_cast<float>(o.fixed_scale);
-      o.count_samples = count_samples_ ? 1u : 0u;
-      o.bins_d = static_cast<double>(s.number_of_bins);
-      o.bins = s.number_of_bins;
-      o.offset = offset;
-      if (!homogeneous) {
-        o.dest_height = (s.position_m[2] - propagation_.min_height) * propagation_.inv_step;
-        o.dest_index = static_cast<uint64_t>(o.dest_height + 0.5);
-        o.dest_n = table_host_[o.dest_index].x + 1.;
-        o.dest_integral = table_host_[o.dest_index].y;
-      }
+      out.push_back(make_observer_cache(
+          s, a, homogeneous, propagation_.min_height, propagation_.inv_step,
+          [&](uint64_t i) { return table_host_[i]; }, deterministic_, limit_, count_samples_, offset));
       offset += static_cast<std::size_t>(s.number_of_bins);
-      out.push_back(o);
     }
     bins_[a] = offset;
   }
@@ -681,9 +662,7 @@ class Accumulator {
       std::vector<double> factors;
       for (auto const& s : snapshots_[a]) {
         max_observer_bins_[a] = std::max<uint64_t>(max_observer_bins_[a], s.number_of_bins);
-        // downloadSet's inverse scale, RadioAccumulator.inl:865-867
-        double const factor = a == 1 ? s.sample_rate_hz : 1.;
-        factors.push_back(limit_ / (kHeadroom * factor));
+        factors.push_back(decode_factor(s, a, limit_));  // downloadSet, RadioAccumulator.inl:865-867
       }
       for (auto const& o : host) offsets.push_back(o.offset);
       offsets.push_back(bins_[a]);

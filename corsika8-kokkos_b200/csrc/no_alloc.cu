@@ -28,6 +28,7 @@
 #include <string>
 
 #include "../../include/c8radio.h"
+#include "host_setup.hpp"
 #include "radio_kernels.cuh"
 
 namespace c8r {
@@ -102,9 +103,8 @@ DeviceSetup const& setup_current_device() {
   return s;
 }
 
-// RadioAccumulator::makeObservers (RadioAccumulator.inl:522-550): the same
-// per-observer constants the accumulator derives, with the same IEEE
-// operations, built 32 at a time on the host stack and copied into scratch.
+// The accumulator's per-observer constants (make_observer_cache), built 32
+// at a time on the host stack and copied into scratch.
 void upload_observers(c8r_config const& config, int algorithm, ObserverCache* device_out,
                       std::size_t& bins, cudaStream_t stream) {
   c8r_observer_snapshot const* snapshots = algorithm == 0 ? config.coreas_observers : config.zhs_observers;
@@ -120,31 +120,11 @@ void upload_observers(c8r_config const& config, int algorithm, ObserverCache* de
     std::size_t const n = std::min(kBlock, count - first);
     for (std::size_t k = 0; k < n; ++k) {
       c8r_observer_snapshot const& s = snapshots[first + k];
-      ObserverCache o;
-      std::memset(&o, 0, sizeof o);
-      o.px = s.position_m[0];
-      o.py = s.position_m[1];
-      o.pz = s.position_m[2];
-      o.start_time = s.start_time_s;
-      o.end_time = s.start_time_s + s.duration_s;
-      o.sample_rate = s.sample_rate_hz;
-      o.resolution = 1. / s.sample_rate_hz;
-      o.wavelength = c8r::kSpeedOfLight / s.sample_rate_hz;
-      double const factor = algorithm == 1 ? s.sample_rate_hz : 1.;
-      o.fixed_scale = fixed ? c8r::kHeadroom * factor / limit : 1.;
-      o.fixed_scale_f = static_cast<float>(o.fixed_scale);
-      o.count_samples = config.count_samples ? 1u : 0u;
-      o.bins_d = static_cast<double>(s.number_of_bins);
-      o.bins = s.number_of_bins;
-      o.offset = offset;
-      if (!homogeneous) {
-        o.dest_height = (s.position_m[2] - p.minimum_height_m) * p.inverse_step_per_m;
-        o.dest_index = static_cast<uint64_t>(o.dest_height + 0.5);
-        o.dest_n = p.refractivity[o.dest_index] + 1.;
-        o.dest_integral = p.integrated_refractivity[o.dest_index];
-      }
+      block[k] = c8r::make_observer_cache(
+          s, algorithm, homogeneous, p.minimum_height_m, p.inverse_step_per_m,
+          [&](uint64_t i) { return make_double2(p.refractivity[i], p.integrated_refractivity[i]); },
+          fixed, limit, config.count_samples != 0, offset);
       offset += static_cast<std::size_t>(s.number_of_bins);
-      block[k] = o;
     }
     // pageable source: the copy has read `block` when the call returns
     check(cudaMemcpyAsync(device_out + first, block, n * sizeof(ObserverCache), cudaMemcpyHostToDevice,

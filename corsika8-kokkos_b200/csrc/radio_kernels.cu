@@ -1019,8 +1019,9 @@ __global__ void __launch_bounds__(kAlgorithm == 1 ? kZhsThreadsMax : kWindowThre
     constexpr int algorithm = kAlgorithm;
     uint64_t const local = item - ev.first_item;
     uint32_t const per_chunk = ev.observer_count[algorithm];
-    uint64_t const chunk = local / per_chunk;
-    uint32_t const oi = static_cast<uint32_t>(local - chunk * per_chunk);
+    uint64_t const slice_chunk = local / per_chunk;
+    uint32_t const oi = static_cast<uint32_t>(local - slice_chunk * per_chunk);
+    uint64_t const chunk = ev.chunk_begin + slice_chunk;
     uint64_t const track_count = *ev.valid_tracks;
     uint64_t const begin = chunk * ev.chunk_size;
     if (begin >= track_count) continue;

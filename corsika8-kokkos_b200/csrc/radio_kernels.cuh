@@ -55,7 +55,7 @@ struct EventPlan {
   uint32_t chunk_size;           // tracks per work item
   uint32_t chunks;
   uint32_t window;               // shared-memory bins per item (<= kernel window)
-  uint32_t pad_;
+  uint32_t chunk_begin;          // first chunk of this plan (a slice of the tracks)
 };
 
 // Persistent windowed launch over a work list of (event, chunk, algorithm,

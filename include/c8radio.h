@@ -34,7 +34,8 @@ enum {
   C8R_LENGTH_ERROR = 5,     /* std::length_error */
   C8R_OVERFLOW_ERROR = 6,   /* std::overflow_error */
   C8R_CUDA_ERROR = 7,       /* CUDA runtime failure (message holds the CUDA string) */
-  C8R_BAD_ALLOC = 8         /* device or pinned host allocation failed */
+  C8R_BAD_ALLOC = 8,        /* device or pinned host allocation failed */
+  C8R_TIMEOUT = 9           /* server: not admitted / not complete within the timeout */
 };
 
 /* ---- record layout: corsika/kokkos/data/ParticleState.hpp:24-44 ----------- */
@@ -311,6 +312,62 @@ int c8r_batch_project(c8r_batch* batch, c8r_accumulator* const* events, size_t c
 int c8r_batch_autotune(c8r_batch* batch, c8r_accumulator* const* events, size_t count,
                        int repetitions, c8r_tuning* best, double* best_ms);
 int c8r_batch_graph_captures(const c8r_batch* batch, unsigned long long* captures);
+
+/* ---- Serving: many showers in flight on one GPU ---------------------------
+ * No reference counterpart (the reference runs one shower per accumulator).
+ * A server reserves one HBM arena of budget_bytes at creation and admits
+ * events against it.  An admitted event keeps its observer constants,
+ * refractivity table, traces and counters resident; its tracks are ingested
+ * into kinematics blocks of block_tracks tracks taken from the arena and
+ * handed back once projected, so an event of any size needs only a few
+ * blocks at a time.  A scheduler thread projects in rounds: each round is one
+ * persistent windowed launch per algorithm over slices of every ready event
+ * (about round_pairs track-antenna pairs, shared evenly among the events), so
+ * events that arrive while others are on the GPU join the next round.  Each
+ * event's traces are the same, bit for bit in fixed-point mode, as those of an
+ * accumulator that projects it alone.  All calls are thread-safe. */
+typedef struct c8r_server c8r_server;
+typedef struct c8r_server_options {
+  uint64_t budget_bytes; /* HBM arena reserved at creation (events, blocks) */
+  uint64_t block_tracks; /* tracks per kinematics block; 0 = 1048576 */
+  uint64_t chunk_tracks; /* tracks per work item; 0 = 16384 (divides block_tracks) */
+  uint64_t round_pairs;  /* track-antenna pairs per round; 0 = 4e8 */
+  uint32_t team_size;    /* threads per windowed CTA; 0 = 512 */
+  uint32_t reserved_[7];
+} c8r_server_options;
+typedef struct c8r_server_event_info {
+  uint64_t records;            /* records added */
+  uint64_t coreas_observers, zhs_observers;
+  uint64_t rounds;             /* rounds that projected part of the event */
+  double open_s, admitted_s, closed_s, completed_s;  /* server clock (s since creation) */
+} c8r_server_event_info;
+typedef struct c8r_server_stats {
+  uint64_t rounds, launches, events_admitted, events_completed, blocks_allocated;
+  uint64_t arena_bytes, arena_used_bytes, arena_peak_bytes;
+  uint64_t work_items;         /* (chunk, antenna) items launched */
+} c8r_server_stats;
+
+int c8r_server_create(const c8r_server_options* options, c8r_server** server);
+void c8r_server_destroy(c8r_server* server);
+const char* c8r_server_last_error(const c8r_server* server);
+/* Admits an event: waits up to timeout_ms (< 0: no limit) until its resident
+ * part and one kinematics block fit the arena (C8R_TIMEOUT otherwise). */
+int c8r_server_open(c8r_server* server, const c8r_config* config, int timeout_ms, uint64_t* event);
+/* Ingests device records on `stream` (ordered with the producer, like
+ * c8r_accumulate_device); waits for a free block when its block is full. */
+int c8r_server_add_device(c8r_server* server, uint64_t event, const c8r_lepton_transport_record* records,
+                          size_t count, size_t extent, void* stream);
+/* No more tracks: the event completes once all its tracks are projected. */
+int c8r_server_close(c8r_server* server, uint64_t event);
+/* C8R_OK once the event is complete, C8R_TIMEOUT after timeout_ms (< 0: no limit). */
+int c8r_server_wait(c8r_server* server, uint64_t event, int timeout_ms);
+/* Copies a complete event's traces to host memory (fixed-point as
+ * c8r_download_fixed, or decoded as c8r_download) and releases the event. */
+int c8r_server_fetch_fixed(c8r_server* server, uint64_t event, long long* coreas_xyz, long long* zhs_xyz,
+                           c8r_counters* counters, c8r_server_event_info* info);
+int c8r_server_fetch(c8r_server* server, uint64_t event, double* coreas_xyz, double* zhs_xyz,
+                     c8r_counters* counters, c8r_server_event_info* info);
+int c8r_server_get_stats(const c8r_server* server, c8r_server_stats* stats);
 
 /* ---- Accumulate without allocating device memory ---------------------------
  * No counterpart in the reference.  For callers that cannot allocate device
