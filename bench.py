@@ -63,6 +63,14 @@ def parse_args():
     p.add_argument("--no-variants", action="store_true",
                    help="skip the FP64 windowed and plain FP64 direct comparison runs")
     p.add_argument("--baseline-segments", type=int, default=100_000)
+    p.add_argument("--no-serving", action="store_true", help="skip the served-stream leg")
+    p.add_argument("--serve-events", type=int, default=40)
+    p.add_argument("--serve-rate", type=float, default=20.0, help="Poisson arrivals per second")
+    p.add_argument("--serve-budget-gb", type=float, default=120.0)
+    p.add_argument("--library-segments", type=int, default=500_000,
+                   help="segments of each of the 15 replayed library showers")
+    p.add_argument("--plain-fraction", type=int, default=8,
+                   help="the plain event-by-event comparison projects 1/N of every event's segments")
     return p.parse_args()
 
 
@@ -321,6 +329,12 @@ def run_ours(args):
                     "sample": f"first {sample.size} of {n} segments x {observers} antennas "
                               f"({bpairs:.3g} pairs), fixed-point CoREAS+ZHS, one pass"}
 
+    serving = None
+    if rank == 0 and world == 1 and not args.no_serving:
+        del device_records
+        torch.cuda.empty_cache()
+        serving = run_serving(pkg, showers, torch, args, local)
+
     if world > 1:
         dist.destroy_process_group()
     if rank != 0:
@@ -341,9 +355,157 @@ def run_ours(args):
         "counters": {k: counters[k] for k in ("valid_tracks", "coreas_contributions",
                                               "zhs_contributions", "zhs_subtracks",
                                               "fixed_point_overflows")},
-        "variants": variants, "peaks": peaks,
+        "variants": variants, "peaks": peaks, "serving": serving,
     }
     print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ served stream
+def run_serving(pkg, showers, torch, args, local: int) -> dict:
+    """The served form: a Poisson stream of batched-workload events with a heavy
+    tail, each event opened on a RadioServer at its arrival time by its own
+    producer thread, its segments added as device records (replayed from a
+    device-resident library of seeded showers), then waited for and fetched
+    (fixed-point traces to host).  Latency = fetch return - scheduled arrival;
+    throughput = all pairs / (last fetch - first arrival).  Beside it, the plain
+    FP64 drop-in (direct kernel, one accumulator per event, event by event) on
+    1/plain_fraction of every event's segments, and the mixed-precision trace
+    error of the served path against FP64 on the smallest events."""
+    import threading
+
+    specs, arrivals = showers.served_event_specs(events=args.serve_events, rate_hz=args.serve_rate)
+    size = args.library_segments
+    library = showers.shower_library(size)
+    itemsize = next(iter(library.values())).itemsize
+    dev = {k: torch.from_numpy(v.view(np.uint8).reshape(-1)).cuda() for k, v in library.items()}
+    configs = [showers.make_config(showers.event_workload(spec)[0], precision=1, kernel=2)
+               for spec in specs]
+    torch.cuda.synchronize()
+    server = pkg.RadioServer(budget_bytes=int(args.serve_budget_gb * 1e9))
+
+    def feed(event, spec, count, stream):
+        base = dev[showers.library_key(spec)].data_ptr()
+        for offset, n in showers.replay_slices(count, size):
+            server.add_device(event, base + offset * itemsize, n, stream=stream)
+
+    # warm-up: one small event (module loads, occupancy queries)
+    warm = server.open(configs[0])
+    feed(warm, specs[0], min(specs[0].segments, 100_000), 0)
+    server.close_event(warm)
+    server.fetch_fixed(warm)
+
+    small = sorted(range(len(specs)), key=lambda k: specs[k].segments * specs[k].antennas)[:3]
+    results = [None] * len(specs)
+    kept = {}
+    errors = []
+    start = time.perf_counter() + 0.1
+
+    def handle(k):
+        try:
+            torch.cuda.set_device(local)
+            stream = torch.cuda.Stream()
+            delay = start + arrivals[k] - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            event = server.open(configs[k])
+            feed(event, specs[k], specs[k].segments, stream.cuda_stream)
+            server.close_event(event)
+            server.wait(event)
+            coreas, zhs, counters, info = server.fetch_fixed(event)
+            done = time.perf_counter()
+            results[k] = {"latency": done - (start + arrivals[k]), "done": done, "info": info,
+                          "overflows": counters["fixed_point_overflows"]}
+            if k in small:
+                kept[k] = (coreas, zhs)
+        except Exception as exc:  # reported below
+            errors.append(f"event {k}: {exc!r}")
+
+    threads = [threading.Thread(target=handle, args=(k,)) for k in range(len(specs))]
+    with ClockSampler(local) as clocks:
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+    stats = server.stats()
+    server.close()
+    if errors:
+        raise RuntimeError("; ".join(errors))
+    pairs = [s.segments * s.antennas for s in specs]
+    latency = np.array([r["latency"] for r in results])
+    makespan = max(r["done"] for r in results) - start
+    served = sum(pairs) / makespan
+    tail = [k for k, s in enumerate(specs) if s.segments == max(x.segments for x in specs)]
+
+    # plain FP64 drop-in, event by event, on a fixed fraction of each event
+    plain_pairs, plain_seconds = 0, 0.0
+    stream = torch.cuda.current_stream()
+    for k, spec in enumerate(specs):
+        count = max(1, spec.segments // args.plain_fraction)
+        wl, _ = showers.event_workload(spec)
+        acc = pkg.RadioAccumulator(showers.make_config(wl, precision=0, kernel=1),
+                                   stream=stream.cuda_stream)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        base = dev[showers.library_key(spec)].data_ptr()
+        for offset, n in showers.replay_slices(count, size):
+            acc.accumulate_lepton_tracks(base + offset * itemsize, n)
+        acc.download_fixed()
+        plain_seconds += time.perf_counter() - t0
+        plain_pairs += count * spec.antennas
+        acc.close()
+    plain = plain_pairs / plain_seconds
+
+    # served (mixed precision) traces against FP64 alone, per antenna trace
+    worst = 0.0
+    traces = 0
+    for k in small:
+        wl, _ = showers.event_workload(specs[k])
+        acc = pkg.RadioAccumulator(showers.make_config(wl, precision=0, kernel=2),
+                                   stream=stream.cuda_stream)
+        base = dev[showers.library_key(specs[k])].data_ptr()
+        for offset, n in showers.replay_slices(specs[k].segments, size):
+            acc.accumulate_lepton_tracks(base + offset * itemsize, n)
+        ref = acc.download_fixed()
+        acc.close()
+        bins = int(wl["observers"]["number_of_bins"][0])
+        for got, want in zip(kept[k], ref[:2]):
+            g = got.astype(np.float64).reshape(3, -1, bins)
+            w = want.astype(np.float64).reshape(3, -1, bins)
+            norm = np.sqrt((w ** 2).sum(axis=(0, 2)))
+            diff = np.sqrt(((g - w) ** 2).sum(axis=(0, 2)))
+            ok = norm > 0
+            traces += int(ok.sum())
+            if ok.any():
+                worst = max(worst, float((diff[ok] / norm[ok]).max()))
+    del dev
+    torch.cuda.empty_cache()
+    pct = lambda a, q: float(np.percentile(a, q))  # noqa: E731
+    others = np.array([latency[k] for k in range(len(specs)) if k not in tail])
+    return {
+        "workload": (f"served_c4: {len(specs)} events, Poisson {args.serve_rate:g}/s, segments "
+                     f"log-uniform 1e5-2e7, 16-300 antennas, zenith 0-60, Xmax 550-850, "
+                     f"{len(tail)} tail events of 5e7 x 300, 4096 bins, CoREAS+ZHS, mixed precision, "
+                     f"fixed point"),
+        "inputs": (f"device-resident replay of 15 seeded library showers ({size} segments each, "
+                   f"nearest zenith/Xmax), added by one producer thread per event"),
+        "budget_gb": args.serve_budget_gb, "events": len(specs), "pairs": int(sum(pairs)),
+        "makespan_s": makespan, "pairs_per_s": served,
+        "offered_pairs_per_s": sum(pairs) / max(float(arrivals[-1]), 1e-9),
+        "latency_s": {"p50": pct(latency, 50), "p95": pct(latency, 95), "p99": pct(latency, 99),
+                      "max": float(latency.max())},
+        "latency_non_tail_s": {"p50": pct(others, 50), "p99": pct(others, 99)},
+        "rounds": stats["rounds"], "launches": stats["launches"],
+        "arena_peak_gb": stats["arena_peak_bytes"] / 1e9,
+        "fixed_point_overflows": int(sum(r["overflows"] for r in results)),
+        "plain_event_by_event": {
+            "pairs_per_s": plain,
+            "sample": (f"every event of the stream, first 1/{args.plain_fraction} of its segments, "
+                       f"FP64 direct kernel, one accumulator per event (accumulate + download_fixed)")},
+        "served_vs_plain": served / plain,
+        "accuracy_vs_fp64": {"max_rel_l2_per_trace": worst, "traces": traces,
+                             "events": "the 3 smallest events of the stream"},
+        "clocks": clocks.summary(),
+    }
 
 
 def run_e2e(pkg, showers, wl, records, precision, kernel, stream, args, torch, barrier,

@@ -60,8 +60,10 @@ std::size_t round_up(std::size_t bytes) { return (bytes + kGranule - 1) / kGranu
 // First-fit sub-allocator over one device reservation, coalescing on release.
 class Arena {
  public:
-  ~Arena() {
+  ~Arena() { free_all(); }
+  void free_all() {
     if (base_) cudaFree(base_);
+    base_ = nullptr;
   }
   void reserve(std::size_t bytes) {
     bytes = bytes / kGranule * kGranule;
@@ -163,6 +165,25 @@ struct Round {
   cudaEvent_t done;
 };
 
+// The current device is per host thread: make the server's device current
+// for the duration of a call and restore the caller's afterwards.
+class DeviceGuard {
+ public:
+  explicit DeviceGuard(int device) {
+    if (cudaGetDevice(&previous_) != cudaSuccess) previous_ = -1;
+    if (previous_ != device) check(cudaSetDevice(device), "cudaSetDevice");
+    else previous_ = -1;
+  }
+  ~DeviceGuard() {
+    if (previous_ >= 0) cudaSetDevice(previous_);
+  }
+  DeviceGuard(DeviceGuard const&) = delete;
+  DeviceGuard& operator=(DeviceGuard const&) = delete;
+
+ private:
+  int previous_ = -1;
+};
+
 class Server {
  public:
   explicit Server(c8r_server_options const& options) {
@@ -200,6 +221,9 @@ class Server {
     memory_cv_.notify_all();
     done_cv_.notify_all();
     if (scheduler_.joinable()) scheduler_.join();
+    int previous = -1;
+    if (cudaGetDevice(&previous) != cudaSuccess || previous == device_) previous = -1;
+    if (previous >= 0) cudaSetDevice(device_);
     cudaStreamSynchronize(compute_);
     for (auto& r : inflight_) cudaEventDestroy(r.done);
     for (auto e : spare_events_) cudaEventDestroy(e);
@@ -210,9 +234,12 @@ class Server {
     cudaStreamDestroy(admit_);
     cudaStreamDestroy(fetch_);
     cudaFree(next_item_);
+    arena_.free_all();
+    if (previous >= 0) cudaSetDevice(previous);
   }
 
   uint64_t open(c8r_config const& config, int timeout_ms) {
+    DeviceGuard guard(device_);
     double const opened = now();
     if (!config.enabled) throw std::invalid_argument("served radio event must be enabled");
     if (c8r_config_validate(&config) != C8R_OK) throw std::invalid_argument(c8r_last_global_error());
@@ -349,6 +376,7 @@ class Server {
 
   void add_device(uint64_t id, c8r_lepton_transport_record const* records, std::size_t count,
                   std::size_t extent, cudaStream_t stream) {
+    DeviceGuard guard(device_);
     if (count > extent) throw std::out_of_range("radio track count exceeds input view");
     if (count != 0 && records == nullptr) throw std::invalid_argument("null device radio track input");
     std::unique_lock<std::mutex> lock(mu_);
@@ -386,6 +414,7 @@ class Server {
   }
 
   void close(uint64_t id) {
+    DeviceGuard guard(device_);
     std::lock_guard<std::mutex> lock(mu_);
     rethrow_failure();
     ServedEvent& ev = find(id);
@@ -424,6 +453,7 @@ class Server {
   // Copies traces (fixed: long long, else decoded doubles) and releases the event.
   void fetch(uint64_t id, void* coreas, void* zhs, bool fixed_out, c8r_counters* counters,
              c8r_server_event_info* info) {
+    DeviceGuard guard(device_);
     std::unique_lock<std::mutex> lock(mu_);
     ServedEvent& ev = find(id);
     if (ev.fetching) throw std::logic_error("radio event already being fetched");
@@ -536,6 +566,7 @@ class Server {
   void run() {
     std::unique_lock<std::mutex> lock(mu_);
     try {
+      check(cudaSetDevice(device_), "cudaSetDevice");
       for (;;) {
         retire_finished();
         complete_finished();

@@ -350,3 +350,56 @@ def event_workload(spec: EventSpec, ground_z_m: float = 1400.0):
     table = flat_atmosphere_table(model, ground_z_m, 30000.0, 1.0)
     gen = dict(zenith_deg=spec.zenith_deg, xmax=spec.xmax, ground_z_m=ground_z_m, model=model)
     return dict(observers=observers, table=table, homogeneous=0.0), gen
+
+
+def served_event_specs(events: int = 40, seed: int = 4242, rate_hz: float = 20.0,
+                       tail_fraction: float = 0.05, tail_segments: int = 50_000_000,
+                       tail_antennas: int = 300, bins: int = 4096):
+    """A served stream: batched-workload events with Poisson arrivals at
+    `rate_hz` and a heavy tail (round(tail_fraction x events) events, at seeded
+    positions, of tail_segments x tail_antennas).  Returns (specs, arrival
+    times in s from the stream start)."""
+    specs = batched_event_specs(events, seed=seed, bins=bins)
+    rng = np.random.Generator(np.random.PCG64(seed + 1))
+    for i in rng.choice(events, int(round(tail_fraction * events)), replace=False):
+        specs[int(i)].segments = tail_segments
+        specs[int(i)].antennas = tail_antennas
+    arrivals = np.cumsum(rng.exponential(1.0 / rate_hz, events))
+    arrivals -= arrivals[0]
+    return specs, arrivals
+
+
+LIBRARY_ZENITHS = (0.0, 15.0, 30.0, 45.0, 60.0)
+LIBRARY_XMAX = (550.0, 700.0, 850.0)
+
+
+def shower_library(segments: int = 500_000, seed: int = 9090, ground_z_m: float = 1400.0) -> dict:
+    """Seeded showers for replayed streams, one per (zenith, Xmax) of
+    LIBRARY_ZENITHS x LIBRARY_XMAX: {(zenith, xmax): records}.  An event
+    replays the library shower nearest its zenith and Xmax, cycling through it
+    when the event has more segments (as a track spool is replayed)."""
+    model = AtmosphereModel()
+    out = {}
+    for i, zenith in enumerate(LIBRARY_ZENITHS):
+        for j, xmax in enumerate(LIBRARY_XMAX):
+            out[(zenith, xmax)] = shower_records(segments, seed=seed + 31 * i + j, zenith_deg=zenith,
+                                                 xmax=xmax, ground_z_m=ground_z_m, model=model)
+    return out
+
+
+def library_key(spec: EventSpec):
+    zenith = min(LIBRARY_ZENITHS, key=lambda z: abs(z - spec.zenith_deg))
+    xmax = min(LIBRARY_XMAX, key=lambda x: abs(x - spec.xmax))
+    return zenith, xmax
+
+
+def replay_slices(total: int, library_size: int):
+    """(offset, count) pieces that cycle through a library shower of
+    library_size records until `total` records are covered."""
+    out, done, offset = [], 0, 0
+    while done < total:
+        n = min(total - done, library_size - offset)
+        out.append((offset, n))
+        done += n
+        offset = (offset + n) % library_size
+    return out
