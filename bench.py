@@ -219,14 +219,8 @@ def run_ours(args):
         if world > 1:
             dist.barrier()
 
-    def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
     pkg, showers, wl, records = build_workload(args.workload, args.segments, seed=1000 + rank)
+    from corsika8_kokkos_b200.sharding import max_over_ranks
     n = records.size
     observers = len(wl["observers"])
     pairs_per_step = n * observers
