@@ -220,6 +220,7 @@ __device__ __forceinline__ Vec3<T> cross(Vec3<T> a, Vec3<T> b) {
 // Per-thread event counters (RadioCounters' projection fields).
 struct Counts {
   unsigned long long coreas = 0, zhs = 0, subtracks = 0, overflows = 0;
+  float mag = 0.f;  // sum of |fixed-point increments| added to a window without checks
 };
 
 }  // namespace c8r

@@ -28,24 +28,32 @@ constexpr double kEmConstant = 1. / (4. * kPi * kVacuumPermittivity * kSpeedOfLi
 
 // ---------------------------------------------------------------- fixed point
 // add_radio_fixed_point, RadioProjection.inl:254-260.
-__device__ __forceinline__ bool to_fixed(double v, ObserverCache const& o, long long& out) {
+// `mag` gains |v scale| (an upper bound of |out| up to half a unit) when the
+// conversion succeeds.
+__device__ __forceinline__ bool to_fixed(double v, ObserverCache const& o, long long& out,
+                                         float& mag) {
   if (o.count_samples) {
     out = 1;
+    mag += 1.f;
     return true;
   }
   double const s = v * o.fixed_scale;
   if (!(fabs(s) < kSignedLimit)) return false;  // also rejects NaN and infinities
   out = __double2ll_rn(s);
+  mag += static_cast<float>(fabs(s));
   return true;
 }
-__device__ __forceinline__ bool to_fixed(float v, ObserverCache const& o, long long& out) {
+__device__ __forceinline__ bool to_fixed(float v, ObserverCache const& o, long long& out,
+                                         float& mag) {
   if (o.count_samples) {
     out = 1;
+    mag += 1.f;
     return true;
   }
   float const s = v * o.fixed_scale_f;
   if (!(fabsf(s) < 9223372036854775808.f)) return false;  // also rejects NaN and infinities
   out = __float2ll_rn(s);
+  mag += fabsf(s);
   return true;
 }
 
@@ -91,7 +99,9 @@ struct GlobalSink {
   __device__ __forceinline__ void addf(int c, uint64_t bin, double v) { atomicAdd(frow[c] + bin, v); }
   // All three components at one bin; false if a conversion failed or an add overflowed.
   __device__ __forceinline__ bool add3(uint64_t bin, long long x, long long y, long long z,
-                                       bool ox, bool oy, bool oz) {
+                                       bool ox, bool oy, bool oz, float mag, float& bound) {
+    (void)mag;
+    (void)bound;
     unsigned long long const px = ox ? atomicAdd(row[0] + bin, static_cast<unsigned long long>(x)) : 0ull;
     unsigned long long const py = oy ? atomicAdd(row[1] + bin, static_cast<unsigned long long>(y)) : 0ull;
     unsigned long long const pz = oz ? atomicAdd(row[2] + bin, static_cast<unsigned long long>(z)) : 0ull;
@@ -127,6 +137,7 @@ struct WindowSink {
   unsigned long long* win;
   double* fwin;
   uint32_t width;
+  bool unchecked;
   unsigned long long* row[3];
   double* frow[3];
   __device__ __forceinline__ bool add(int c, uint64_t bin, long long v) {
@@ -141,11 +152,21 @@ struct WindowSink {
     else
       atomicAdd(frow[c] + bin, v);
   }
+  // unchecked: window adds whose results are not read; `bound` then gains
+  // |x| + |y| + |z| (as `mag`), and the kernel checks afterwards that no
+  // partial sum of the window can have left the int64 range.
   __device__ __forceinline__ bool add3(uint64_t bin, long long x, long long y, long long z,
-                                       bool ox, bool oy, bool oz) {
+                                       bool ox, bool oy, bool oz, float mag, float& bound) {
     if (bin >= width)
       return spill3(row[0] + bin, row[1] + bin, row[2] + bin, x, y, z, ox, oy, oz);
     unsigned long long* const w = win + bin;
+    if (unchecked) {
+      if (ox) atomicAdd(w, static_cast<unsigned long long>(x));
+      if (oy) atomicAdd(w + width, static_cast<unsigned long long>(y));
+      if (oz) atomicAdd(w + 2 * width, static_cast<unsigned long long>(z));
+      bound += mag;
+      return ox && oy && oz;
+    }
     unsigned long long const px = ox ? atomicAdd(w, static_cast<unsigned long long>(x)) : 0ull;
     unsigned long long const py = oy ? atomicAdd(w + width, static_cast<unsigned long long>(y)) : 0ull;
     unsigned long long const pz =
@@ -183,16 +204,18 @@ struct Deposit {
   Vec3<Amp> value;
   long long ix, iy, iz;
   bool okx, oky, okz;
+  float mag;  // |scaled components| that converted
 };
 
 template <bool kFixed, class Amp>
 __device__ __forceinline__ Deposit<Amp> make_deposit(ObserverCache const& o, Vec3<Amp> v) {
   Deposit<Amp> d;
   d.value = v;
+  d.mag = 0.f;
   if (kFixed) {
-    d.okx = to_fixed(v.x, o, d.ix);
-    d.oky = to_fixed(v.y, o, d.iy);
-    d.okz = to_fixed(v.z, o, d.iz);
+    d.okx = to_fixed(v.x, o, d.ix, d.mag);
+    d.oky = to_fixed(v.y, o, d.iy, d.mag);
+    d.okz = to_fixed(v.z, o, d.iz, d.mag);
   }
   return d;
 }
@@ -200,11 +223,12 @@ __device__ __forceinline__ Deposit<Amp> make_deposit(ObserverCache const& o, Vec
 template <bool kPotential, bool kFixed, class Amp, class Sink>
 __device__ __forceinline__ void deposit(ObserverCache const& o, Sink& sink, double t,
                                         Deposit<Amp> const& d, unsigned long long& contributions,
-                                        unsigned long long& overflows) {
+                                        unsigned long long& overflows, float& bound) {
   uint64_t bin;
   if (!sample_bin<kPotential>(o, t, bin)) return;
   if (kFixed) {
-    if (!sink.add3(bin, d.okx ? d.ix : 0, d.oky ? d.iy : 0, d.okz ? d.iz : 0, d.okx, d.oky, d.okz)) {
+    if (!sink.add3(bin, d.okx ? d.ix : 0, d.oky ? d.iy : 0, d.okz ? d.iz : 0, d.okx, d.oky, d.okz,
+                   d.mag, bound)) {
       ++overflows;
       return;
     }
@@ -218,15 +242,13 @@ __device__ __forceinline__ void deposit(ObserverCache const& o, Sink& sink, doub
 template <bool kPotential, bool kFixed, class Amp, class Sink>
 __device__ __forceinline__ void add_sample(ObserverCache const& o, Sink& sink, double t,
                                            Vec3<Amp> v, unsigned long long& contributions,
-                                           unsigned long long& overflows) {
+                                           unsigned long long& overflows, float& bound) {
   uint64_t bin;
   if (!sample_bin<kPotential>(o, t, bin)) return;
+  Deposit<Amp> const d = make_deposit<kFixed>(o, v);
   if (kFixed) {
-    long long ix = 0, iy = 0, iz = 0;
-    bool const ox = to_fixed(v.x, o, ix);
-    bool const oy = to_fixed(v.y, o, iy);
-    bool const oz = to_fixed(v.z, o, iz);
-    if (!sink.add3(bin, ox ? ix : 0, oy ? iy : 0, oz ? iz : 0, ox, oy, oz)) {
+    if (!sink.add3(bin, d.okx ? d.ix : 0, d.oky ? d.iy : 0, d.okz ? d.iz : 0, d.okx, d.oky, d.okz,
+                   d.mag, bound)) {
       ++overflows;
       return;
     }
@@ -240,9 +262,10 @@ __device__ __forceinline__ void add_sample(ObserverCache const& o, Sink& sink, d
 template <bool kFixed, class Amp, class Sink>
 __device__ __forceinline__ void deposit_bin(Sink& sink, uint64_t bin, Deposit<Amp> const& d,
                                             unsigned long long& contributions,
-                                            unsigned long long& overflows) {
+                                            unsigned long long& overflows, float& bound) {
   if (kFixed) {
-    if (!sink.add3(bin, d.okx ? d.ix : 0, d.oky ? d.iy : 0, d.okz ? d.iz : 0, d.okx, d.oky, d.okz)) {
+    if (!sink.add3(bin, d.okx ? d.ix : 0, d.oky ? d.iy : 0, d.okz ? d.iz : 0, d.okx, d.oky, d.okz,
+                   d.mag, bound)) {
       ++overflows;
       return;
     }
@@ -302,8 +325,8 @@ __device__ __noinline__ Counts coreas_near_cone(Track const t, Propagation const
     fend = scaled(fend, s);
     separate_same_bin(sr, er, res, true);
   }
-  add_sample<false, kFixed>(o, sink, sr, fstart, c.coreas, c.overflows);
-  add_sample<false, kFixed>(o, sink, er, fend, c.coreas, c.overflows);
+  add_sample<false, kFixed>(o, sink, sr, fstart, c.coreas, c.overflows, c.mag);
+  add_sample<false, kFixed>(o, sink, er, fend, c.coreas, c.overflows, c.mag);
   return c;
 }
 
@@ -326,6 +349,7 @@ __device__ __forceinline__ void coreas_pair(Track const& t, Propagation const& p
     Counts const d = coreas_near_cone<kFixed, Amp>(t, p, o, sink, sr < er);
     c.coreas += d.coreas;
     c.overflows += d.overflows;
+    c.mag += d.mag;
     return;
   }
 
@@ -345,8 +369,8 @@ __device__ __forceinline__ void coreas_pair(Track const& t, Propagation const& p
       separate_same_bin(sr, er, res, false);
     }
   }
-  add_sample<false, kFixed>(o, sink, sr, fstart, c.coreas, c.overflows);
-  add_sample<false, kFixed>(o, sink, er, fend, c.coreas, c.overflows);
+  add_sample<false, kFixed>(o, sink, sr, fstart, c.coreas, c.overflows, c.mag);
+  add_sample<false, kFixed>(o, sink, er, fend, c.coreas, c.overflows, c.mag);
 }
 
 // The exact pair out of line: the filtered path's fallback.
@@ -415,8 +439,8 @@ __device__ __forceinline__ bool coreas_common(Track const& t, Propagation const&
       separate_same_bin(sr, er, res, false);
     }
   }
-  add_sample<false, kFixed>(o, sink, sr, fstart, c.coreas, c.overflows);
-  add_sample<false, kFixed>(o, sink, er, fend, c.coreas, c.overflows);
+  add_sample<false, kFixed>(o, sink, sr, fstart, c.coreas, c.overflows, c.mag);
+  add_sample<false, kFixed>(o, sink, er, fend, c.coreas, c.overflows, c.mag);
   return true;
 }
 
@@ -441,7 +465,7 @@ __device__ __noinline__ Counts zhs_indexed_bins(ObserverCache const& o, Sink sin
     if (hi > nb) hi = nb;
   }
   for (int index = lo; index < hi; ++index)
-    deposit<true, kFixed>(o, sink, d1 + static_cast<double>(index) / fs, mid, c.zhs, c.overflows);
+    deposit<true, kFixed>(o, sink, d1 + static_cast<double>(index) / fs, mid, c.zhs, c.overflows, c.mag);
   return c;
 }
 
@@ -461,7 +485,7 @@ __device__ __noinline__ Counts zhs_multi_tail(ObserverCache const& o, Sink sink,
   double const frac_first = fabs(sb + 0.5 - x1);
   add_sample<true, kFixed>(o, sink, d1,
                            scaled(perp, amp_div(static_cast<Amp>(sc * frac_first), static_cast<Amp>(dd))),
-                           c.zhs, c.overflows);
+                           c.zhs, c.overflows, c.mag);
   if (nb > 1) {
     Deposit<Amp> const mid =
         make_deposit<kFixed>(o, scaled(perp, amp_div(static_cast<Amp>(mc), static_cast<Amp>(dd))));
@@ -489,13 +513,14 @@ __device__ __noinline__ Counts zhs_multi_tail(ObserverCache const& o, Sink sink,
           }
         } else {
           for (uint32_t j = 0; j < count; ++j)
-            deposit_bin<kFixed>(sink, first + j, mid, c.zhs, c.overflows);
+            deposit_bin<kFixed>(sink, first + j, mid, c.zhs, c.overflows, c.mag);
         }
       }
     } else {
       Counts const d = zhs_indexed_bins<kFixed, Amp>(o, sink, d1, x1, nb, mid);
       c.zhs += d.zhs;
       c.overflows += d.overflows;
+      c.mag += d.mag;
     }
   }
   return c;
@@ -589,7 +614,7 @@ __device__ __forceinline__ bool zhs_segment(double p1x, double p1y, double p1z, 
   add_sample<true, kFixed>(o, sink, d2,
                            scaled(perp, amp_div(static_cast<Amp>(sc * frac_last),
                                                 static_cast<Amp>(den_last))),
-                           c.zhs, c.overflows);
+                           c.zhs, c.overflows, c.mag);
   if (single) return true;
   PendingRange run;
   run.count = 0;
@@ -598,8 +623,177 @@ __device__ __forceinline__ bool zhs_segment(double p1x, double p1y, double p1z, 
       pending != nullptr && pending->count == 0, run);
   c.zhs += d.zhs;
   c.overflows += d.overflows;
+  c.mag += d.mag;
   if (run.count) *pending = run;
   return true;
+}
+
+// The samples of one ZHS segment, staged for the warp (windowed kernel): the
+// in-range bins [start, start + count) of its first sample and intermediate
+// bins (value perp * first at `start` when flag bit 0, perp * mid elsewhere)
+// and its last sample at last_bin (flag bit 1).  Bins are consecutive there
+// because the segment is staged only when its intermediate bins are
+// nearest(x1) + i (the consecutive-run test of zhs_segment).
+template <class Amp>
+struct StagedSegment {
+  Vec3<Amp> perp;
+  Amp first, mid, last;
+  uint32_t start, count, last_bin, flags;
+};
+
+// accumulate_zhs_segment (RadioProjection.inl:412-480) with every decision of
+// zhs_segment<kRuns = true, kFilter>, its samples staged instead of
+// deposited.  Returns false, staging nothing, when the segment needs the
+// per-index binning or (kFilter) an exact evaluation, or when the trace has
+// 2^26 bins or more (staged counts then stay far inside 32 bits per warp).
+template <bool kFilter, class Amp>
+__device__ __forceinline__ bool zhs_stage(double p1x, double p1y, double p1z, double p2x,
+                                          double p2y, double p2z, double t1, double t2,
+                                          Track const& t, Propagation const& p,
+                                          ObserverCache const& o, bool subdivided,
+                                          StagedSegment<Amp>& out) {
+  if (!(o.bins_d < 67108864.0)) return false;
+  double const mx = (p1x + p2x) * 0.5, my = (p1y + p2y) * 0.5, mz = (p1z + p2z) * 0.5;
+  Path const path = propagate<true, kFilter>(p, o, mx, my, mz);
+  double const bk = t.bx * path.kx + t.by * path.ky + t.bz * path.kz;
+  double const nbk = path.n_src * bk;
+  double const mt = (t1 + t2) * 0.5;
+  double d1 = t1 + path.time - nbk * (t1 - mt);
+  double d2 = t2 + path.time - nbk * (t2 - mt);
+  double e_d = 0.;
+  if (kFilter) {
+    double const beta1 = fabs(t.bx) + fabs(t.by) + fabs(t.bz) + 1.;
+    double const e_nbk = path.n_src * beta1 * 0x1p-47 + 0x1p-50;
+    double const h = fabs(t1 - mt) + fabs(t2 - mt);
+    e_d = e_nbk * h + 0x1p-50 * (fabs(t1 + path.time) + fabs(t2 + path.time) + fabs(nbk) * h);
+  }
+  double sign = 1.;
+  if (d1 > d2) {
+    double const swap = d1;
+    d1 = d2;
+    d2 = swap;
+    sign = -1.;
+  }
+  double const fs = o.sample_rate;
+  double const x1 = (d1 - o.start_time) * fs;
+  double const x2 = (d2 - o.start_time) * fs;
+  double const sb = floor(x1 + 0.5);
+  double const eb = floor(x2 + 0.5);
+  double const den = 1. - nbk;
+  int const nb = x86_int(eb - sb);
+  double const f1 = fabs(x1 - floor(x1) - 0.5);
+  double const mag = fabs(x1) + static_cast<double>(nb) + fabs(d1 * fs) + fabs(o.start_time * fs) + 2.;
+  bool run_ok = mag < 0x1p50 && f1 > mag * 0x1p-48;
+  if (kFilter) {
+    double const e_x = (e_d + 0x1p-50 * (fabs(d1) + fabs(d2) + 2. * fabs(o.start_time))) * fs +
+                       0x1p-50 * (fabs(x1) + fabs(x2));
+    double const f2 = fabs(x2 - floor(x2) - 0.5);
+    run_ok = run_ok && f1 > mag * 0x1p-48 + e_x;
+    bool const ambiguous = fabs(d1 - d2) <= 2. * e_d || fabs(den) < 1.e-6 ||
+                           f1 <= e_x + 0x1p-50 * (fabs(x1) + 1.) ||
+                           f2 <= e_x + 0x1p-50 * (fabs(x2) + 1.) || (nb > 1 && !run_ok);
+    if (ambiguous) return false;
+  } else if (nb > 1 && !run_ok) {
+    return false;
+  }
+  Vec3<Amp> const k{static_cast<Amp>(path.kx), static_cast<Amp>(path.ky), static_cast<Amp>(path.kz)};
+  Vec3<Amp> const beta{static_cast<Amp>(t.bx), static_cast<Amp>(t.by), static_cast<Amp>(t.bz)};
+  out.perp = cross(k, cross(beta, k));
+  double const sc = sign * t.constant;
+  double const dd = den * path.dist;
+  bool const single = sb == eb;
+  bool const tiny = !(fabs(den) > 1.e-15);
+  double const frac_last = single ? (tiny ? (t2 - t1) * fs : fabs(d2 * fs - d1 * fs))
+                                  : fabs(x2 + 0.5 - eb);
+  double const den_last = single && tiny ? path.dist : dd;
+  out.last = amp_div(static_cast<Amp>(sc * frac_last), static_cast<Amp>(den_last));
+  out.flags = 0u;
+  out.start = 0u;
+  out.count = 0u;
+  out.last_bin = 0u;
+  // last sample, add_sample(detection_time2): bin nearest((d2 - t0) fs) = nearest(x2)
+  double const bv2 = nearest_bin(x2);
+  if (bv2 >= 0. && bv2 < o.bins_d) {
+    out.last_bin = static_cast<uint32_t>(bv2);
+    out.flags = 2u;
+  }
+  if (single) return true;
+  double const frac_first = fabs(sb + 0.5 - x1);
+  out.first = amp_div(static_cast<Amp>(sc * frac_first), static_cast<Amp>(dd));
+  double const mc = (subdivided ? 1. : sign) * t.constant;
+  out.mid = amp_div(static_cast<Amp>(mc), static_cast<Amp>(dd));
+  // first sample, add_sample(detection_time1): bin nearest(x1)
+  double const bv1 = nearest_bin(x1);
+  bool const first_in = bv1 >= 0. && bv1 < o.bins_d;
+  if (first_in) {
+    out.start = static_cast<uint32_t>(bv1);
+    out.count = 1u;
+    out.flags |= 1u;
+  }
+  if (nb > 1) {  // intermediate bins b1 + i, i in [1, nb), clipped to the trace
+    long long const b1 = static_cast<long long>(floor(x1)) + (x1 - floor(x1) >= 0.5 ? 1 : 0);
+    long long lo = 1, hi = nb;
+    if (-b1 > lo) lo = -b1;
+    long long const top = static_cast<long long>(o.bins) - b1;
+    if (top < hi) hi = top;
+    if (hi > lo) {
+      if (first_in) {  // b1 = nearest(x1) >= 0, so lo = 1: one run from the first sample
+        out.count = static_cast<uint32_t>(1 + (hi - lo));
+      } else {
+        out.start = static_cast<uint32_t>(b1 + lo);
+        out.count = static_cast<uint32_t>(hi - lo);
+      }
+    }
+  }
+  return true;
+}
+
+// Deposits the staged segments of a warp: every lane takes one bin of the
+// flattened list (lane order, then bin order) per step.  Every lane of the
+// warp calls it; `staging` is the warp's 32 slots in shared memory.
+template <bool kFixed, class Amp, class Sink>
+__device__ __forceinline__ void deposit_staged(StagedSegment<Amp>* staging,
+                                               StagedSegment<Amp> const& seg,
+                                               ObserverCache const& o, Sink& sink, Counts& c) {
+  unsigned const lane = threadIdx.x & 31u;
+  uint32_t const cnt = seg.count + ((seg.flags >> 1) & 1u);
+  uint32_t incl = cnt;
+#pragma unroll
+  for (unsigned d = 1; d < 32u; d <<= 1) {
+    uint32_t const v = __shfl_up_sync(0xffffffffu, incl, d);
+    if (lane >= d) incl += v;
+  }
+  uint32_t const total = __shfl_sync(0xffffffffu, incl, 31);
+  if (total == 0u) return;
+  staging[lane] = seg;
+  __syncwarp();
+  uint32_t const before_mine = incl - cnt;
+  for (uint32_t base = 0; base < total; base += 32u) {
+    uint32_t const j = base + lane;
+    uint32_t owner = 0;
+#pragma unroll
+    for (uint32_t step = 16; step >= 1u; step >>= 1) {
+      uint32_t const v = __shfl_sync(0xffffffffu, incl, owner + step - 1u);
+      if (v <= j) owner += step;
+    }
+    uint32_t const before = __shfl_sync(0xffffffffu, before_mine, owner & 31u);
+    if (j < total) {
+      StagedSegment<Amp> const& g = staging[owner];
+      uint32_t const k = j - before;
+      uint32_t bin;
+      Amp scale;
+      if (k < g.count) {
+        bin = g.start + k;
+        scale = (k == 0u && (g.flags & 1u)) ? g.first : g.mid;
+      } else {
+        bin = g.last_bin;
+        scale = g.last;
+      }
+      deposit_bin<kFixed>(sink, bin, make_deposit<kFixed>(o, scaled(g.perp, scale)), c.zhs,
+                          c.overflows, c.mag);
+    }
+  }
+  __syncwarp();
 }
 
 // accumulate_zhs, RadioProjection.inl:483-529, every decision exact.
@@ -658,11 +852,11 @@ __device__ __noinline__ Counts zhs_pair_exact(Track const t, Propagation const& 
   return c;
 }
 
-// The common ZHS pair of the windowed kernel: one undivided segment.  Returns
-// false, having deposited nothing, when the track is subdivided (Fraunhofer
-// number above 1, or refinement), when (kFilter) the Fraunhofer test is not
-// surely below 1, or when the filtered segment is ambiguous; the kernel then
-// defers the pair to zhs_pair_exact.
+// The common ZHS pair of the windowed kernel: one undivided segment, staged
+// for the warp's cooperative deposit.  Returns false, staging nothing, when
+// the track is subdivided (Fraunhofer number above 1, or refinement), when
+// (kFilter) the Fraunhofer test is not surely below 1, or when zhs_stage
+// declines the segment; the kernel then defers the pair to zhs_pair_exact.
 //
 // kFilter: F is estimated in FP32 as sin^2(theta) K with
 // sin^2 = |beta x d|^2 / (|beta|^2 |d|^2) and K = 2 pi L^2 / (|d| lambda); its
@@ -670,10 +864,10 @@ __device__ __noinline__ Counts zhs_pair_exact(Track const t, Propagation const& 
 // 1e-12 K (cross-product cancellation and the FP32 roundings; used with a 4x
 // margin), so an estimate surely below 1 decides "one segment" exactly as the
 // reference does.
-template <bool kFixed, bool kFilter, class Amp, class Sink>
+template <bool kFilter, class Amp>
 __device__ __forceinline__ bool zhs_common(Track const& t, Propagation const& p,
-                                           ObserverCache const& o, Sink& sink, Counts& c,
-                                           PendingRange* pending) {
+                                           ObserverCache const& o, Counts& c,
+                                           StagedSegment<Amp>& seg) {
   if (p.refinement != 1u) return false;
   double const mx = (t.sx + t.ex) * 0.5, my = (t.sy + t.ey) * 0.5, mz = (t.sz + t.ez) * 0.5;
   if (kFilter) {
@@ -697,10 +891,9 @@ __device__ __forceinline__ bool zhs_common(Track const& t, Propagation const& p,
     double const fraunhofer = s2 * t.length * t.length / pm.dist / o.wavelength * 2. * kPi;
     if (fraunhofer > 1.) return false;
   }
-  if (!zhs_segment<kFixed, true, kFilter, Amp>(t.sx, t.sy, t.sz, t.sx + (t.ex - t.sx),
-                                               t.sy + (t.ey - t.sy), t.sz + (t.ez - t.sz), t.ts,
-                                               t.ts + (t.te - t.ts), t, p, o, sink, c, false,
-                                               pending))
+  if (!zhs_stage<kFilter, Amp>(t.sx, t.sy, t.sz, t.sx + (t.ex - t.sx), t.sy + (t.ey - t.sy),
+                               t.sz + (t.ez - t.sz), t.ts, t.ts + (t.te - t.ts), t, p, o, false,
+                               seg))
     return false;
   c.subtracks += 1ull;
   return true;
@@ -960,35 +1153,9 @@ constexpr int kWindowThreadsMax = 512;
 // 384-thread CTAs (up to 168 registers, no spills).
 constexpr int kZhsThreadsMax = 384;
 constexpr unsigned kWarpQueue = 64;  // entries per warp: < 32 kept + 32 pushed per round
-
-// Each lane's pending run of consecutive ZHS bins is deposited by the whole
-// warp, 32 bins per step.  Every lane of the warp must call it.
-template <bool kFixed, class Sink>
-__device__ __forceinline__ void deposit_runs(Sink& sink, PendingRange const& run, Counts& c) {
-  unsigned mask = __ballot_sync(0xffffffffu, run.count != 0);
-  unsigned const lane = threadIdx.x & 31u;
-  while (mask) {
-    int const src = __ffs(mask) - 1;
-    mask &= mask - 1;
-    uint64_t const first = __shfl_sync(0xffffffffu, run.bin, src);
-    uint32_t const count = __shfl_sync(0xffffffffu, run.count, src);
-    long long const vx = __shfl_sync(0xffffffffu, run.v[0], src);
-    long long const vy = __shfl_sync(0xffffffffu, run.v[1], src);
-    long long const vz = __shfl_sync(0xffffffffu, run.v[2], src);
-    for (uint32_t k = lane; k < count; k += 32u) {
-      uint64_t const bin = first + k;
-      if (kFixed) {
-        if (sink.add3(bin, vx, vy, vz, true, true, true))
-          ++c.zhs;
-        else
-          ++c.overflows;
-      } else {
-        sink.addf3(bin, __longlong_as_double(vx), __longlong_as_double(vy), __longlong_as_double(vz));
-        ++c.zhs;
-      }
-    }
-  }
-}
+constexpr size_t kQueueBytes = (kWindowThreadsMax / 32) * kWarpQueue * sizeof(unsigned);
+// staging slots of the ZHS kernel: 32 per warp, sized for the FP64 amplitudes
+constexpr size_t kStagingBytes = (kZhsThreadsMax / 32) * 32 * sizeof(StagedSegment<double>);
 
 __device__ __forceinline__ uint32_t find_event(EventPlan const* events, uint32_t n, uint64_t item) {
   uint32_t lo = 0, hi = n;  // last event with first_item <= item
@@ -1008,6 +1175,7 @@ __global__ void __launch_bounds__(kAlgorithm == 1 ? kZhsThreadsMax : kWindowThre
   extern __shared__ __align__(16) unsigned long long window[];
   __shared__ unsigned long long item_shared;
   __shared__ ObserverCache observer;
+  __shared__ float window_bound;
   Counts c;
   for (;;) {
     __syncthreads();
@@ -1031,8 +1199,9 @@ __global__ void __launch_bounds__(kAlgorithm == 1 ? kZhsThreadsMax : kWindowThre
     uint64_t const bins = ev.observers[algorithm][oi].bins;
     uint32_t const width = static_cast<uint32_t>(bins < ev.window ? bins : ev.window);
 
-    // zero the window (3 rows of width bins)
+    // zero the window (3 rows of width bins); the barrier also publishes `observer`
     for (uint32_t j = threadIdx.x; j < 3 * width; j += blockDim.x) window[j] = 0ull;
+    if (threadIdx.x == 0) window_bound = 0.f;
     __syncthreads();
 
     WindowSink sink;
@@ -1052,8 +1221,15 @@ __global__ void __launch_bounds__(kAlgorithm == 1 ? kZhsThreadsMax : kWindowThre
     unsigned* const queue =
         reinterpret_cast<unsigned*>(window + 3 * static_cast<size_t>(plan.window)) +
         (threadIdx.x >> 5) * kWarpQueue;
+    // per-warp staging slots of the ZHS kernel's cooperative deposit
+    StagedSegment<Amp>* const staging =
+        reinterpret_cast<StagedSegment<Amp>*>(
+            reinterpret_cast<unsigned char*>(window + 3 * static_cast<size_t>(plan.window)) +
+            kQueueBytes) +
+        (threadIdx.x >> 5) * 32u;
     unsigned const lane = threadIdx.x & 31u;
     unsigned queued = 0;  // warp-uniform
+    Counts const saved = c;
     auto drain = [&](unsigned from, unsigned count) {
       if (lane < count) {
         Track const t = load_track(ev.tracks, ev.stride, begin + queue[from + lane]);
@@ -1063,34 +1239,60 @@ __global__ void __launch_bounds__(kAlgorithm == 1 ? kZhsThreadsMax : kWindowThre
         c.zhs += d.zhs;
         c.subtracks += d.subtracks;
         c.overflows += d.overflows;
+        c.mag += d.mag;
       }
       __syncwarp();
     };
-    for (uint64_t base = begin; base < end; base += blockDim.x) {
-      uint64_t const i = base + threadIdx.x;
-      bool deferred = false;
-      PendingRange run;
-      run.count = 0;
-      if (i < end) {
-        Track const t = load_track(ev.tracks, ev.stride, i);
-        bool const done =
-            kAlgorithm == 0 ? coreas_common<kFixed, kFilter, Amp>(t, ev.propagation, o, sink, c)
-                            : zhs_common<kFixed, kFilter, Amp>(t, ev.propagation, o, sink, c, &run);
-        deferred = !done;
+    // Fixed point, whole trace in the window: the window takes unchecked
+    // adds, and `c.mag` bounds the sum of |increments| of this thread.  If the
+    // block's bound stays below 2^61 (the FP32 sums are off by a factor below
+    // 1 + 2^-2 for fewer than 2^22 adds a thread), no partial sum of any bin
+    // can have left the int64 range in any order, so no add overflowed; else
+    // the item is run again with checked adds.  Bins past the window and the
+    // flush below are always checked.
+    for (int attempt = 0;; ++attempt) {
+      if (attempt > 0) {
+        for (uint32_t j = threadIdx.x; j < 3 * width; j += blockDim.x) window[j] = 0ull;
+        __syncthreads();
       }
-      if (kAlgorithm == 1) deposit_runs<kFixed>(sink, run, c);
-      unsigned const ballot = __ballot_sync(0xffffffffu, deferred);
-      if (deferred)
-        queue[queued + __popc(ballot & ((1u << lane) - 1u))] = static_cast<unsigned>(i - begin);
-      queued += __popc(ballot);
-      __syncwarp();
-      if (queued >= 32u) {
-        queued -= 32u;
-        drain(queued, 32u);
+      sink.unchecked = kFixed && attempt == 0 && bins <= width;
+      c.mag = 0.f;
+      queued = 0;
+      for (uint64_t base = begin; base < end; base += blockDim.x) {
+        uint64_t const i = base + threadIdx.x;
+        bool deferred = false;
+        StagedSegment<Amp> seg;
+        seg.count = 0u;
+        seg.flags = 0u;
+        if (i < end) {
+          Track const t = load_track(ev.tracks, ev.stride, i);
+          bool const done =
+              kAlgorithm == 0 ? coreas_common<kFixed, kFilter, Amp>(t, ev.propagation, o, sink, c)
+                              : zhs_common<kFilter, Amp>(t, ev.propagation, o, c, seg);
+          deferred = !done;
+        }
+        if (kAlgorithm == 1) deposit_staged<kFixed>(staging, seg, o, sink, c);
+        unsigned const ballot = __ballot_sync(0xffffffffu, deferred);
+        if (deferred)
+          queue[queued + __popc(ballot & ((1u << lane) - 1u))] = static_cast<unsigned>(i - begin);
+        queued += __popc(ballot);
+        __syncwarp();
+        if (queued >= 32u) {
+          queued -= 32u;
+          drain(queued, 32u);
+        }
       }
+      if (queued) drain(0u, queued);
+      __syncthreads();
+      if (!sink.unchecked) break;
+      float const thread_bound = static_cast<float>(warp_sum(static_cast<double>(c.mag)));
+      if (lane == 0) atomicAdd(&window_bound, thread_bound);
+      __syncthreads();
+      float const block_bound = window_bound;
+      __syncthreads();
+      if (block_bound < 0x1p61f) break;
+      c = saved;
     }
-    if (queued) drain(0u, queued);
-    __syncthreads();
 
     // flush: non-zero bins, checked global adds
     for (uint32_t j = threadIdx.x; j < 3 * width; j += blockDim.x) {
@@ -1147,15 +1349,16 @@ cudaError_t direct_dispatch(EventPlan const& ev, uint64_t bound, bool coreas, bo
   return cudaGetLastError();
 }
 
-size_t windowed_smem_bytes(uint32_t window) {
-  return static_cast<size_t>(window) * 3 * sizeof(unsigned long long) +
-         (kWindowThreadsMax / 32) * kWarpQueue * sizeof(unsigned);
+// window rows | per-warp deferral queues | (ZHS) per-warp staging slots
+size_t windowed_smem_bytes(uint32_t window, int algorithm) {
+  return static_cast<size_t>(window) * 3 * sizeof(unsigned long long) + kQueueBytes +
+         (algorithm == 1 ? kStagingBytes : 0);
 }
 
 template <bool kFixed, class Amp, int kAlgorithm>
 cudaError_t windowed_dispatch_algorithm(WorkPlan const& plan, int ctas, int threads,
                                         cudaStream_t stream) {
-  size_t const bytes = windowed_smem_bytes(plan.window);
+  size_t const bytes = windowed_smem_bytes(plan.window, kAlgorithm);
   cudaError_t err = cudaFuncSetAttribute(windowed_kernel<kFixed, Amp, kAlgorithm>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(bytes));
@@ -1174,17 +1377,17 @@ cudaError_t windowed_dispatch(WorkPlan const& plan, int ctas, int threads, cudaS
 
 template <bool kFixed, class Amp>
 int ctas_per_sm(int window, int threads) {
-  size_t const bytes = windowed_smem_bytes(static_cast<uint32_t>(window));
   int worst = 1 << 30;
-  auto probe = [&](auto kernel, int block) {
+  auto probe = [&](auto kernel, int block, int algorithm) {
+    size_t const bytes = windowed_smem_bytes(static_cast<uint32_t>(window), algorithm);
     cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
     int blocks = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, block, bytes) != cudaSuccess)
       blocks = 0;
     worst = blocks < worst ? blocks : worst;
   };
-  probe(windowed_kernel<kFixed, Amp, 0>, threads);
-  probe(windowed_kernel<kFixed, Amp, 1>, threads > kZhsThreadsMax ? kZhsThreadsMax : threads);
+  probe(windowed_kernel<kFixed, Amp, 0>, threads, 0);
+  probe(windowed_kernel<kFixed, Amp, 1>, threads > kZhsThreadsMax ? kZhsThreadsMax : threads, 1);
   return worst;
 }
 
@@ -1226,7 +1429,7 @@ int windowed_max_bins(int device) {
   int optin = 0;
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
   // static shared memory of the kernel is a few hundred bytes; keep 1 KiB spare
-  int const usable = optin - 1024 - static_cast<int>((kWindowThreadsMax / 32) * kWarpQueue * sizeof(unsigned));
+  int const usable = optin - 1024 - static_cast<int>(kQueueBytes + kStagingBytes);
   return usable > 0 ? usable / static_cast<int>(3 * sizeof(unsigned long long)) : 0;
 }
 

@@ -258,6 +258,33 @@ def test_fixed_point_overflow_is_reported(pkg, showers, torch_cuda, kernel):
     acc.close()
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_window_rerun_near_the_fixed_point_limit(pkg, oracle, showers, torch_cuda, precision):
+    """A limit of 1.5x the largest |trace| value: the largest bin then holds
+    2^62/1.5 > 2^61 in fixed point, so its window's bound on the sum of
+    |increments| trips and that item is projected again with checked adds,
+    while every final sum still fits in int64.  The traces equal those of
+    256-track items (bounds far lower) and, in FP64, the oracle's."""
+    wl, records = _workload_records(showers, "plain_c0", 20_000, seed=12)
+    floating = showers.make_config(wl, deterministic=False)
+    coreas, zhs, _ = oracle.restatement().project(floating, records, threads=8)
+    fs = float(wl["observers"]["sample_rate_hz"][0])
+    peak = max(np.abs(coreas).max(), fs * np.abs(zhs).max())
+    config = showers.make_config(wl, precision=precision, kernel=2)
+    config.fixed_point_field_limit_v_per_m = 1.5 * peak
+    # one item holds every track of an antenna, so the largest bin's whole sum is in one window
+    got = gpu_project(pkg, torch_cuda, config, records,
+                      tuning=pkg.TuningParameters(track_tile_size=32768))
+    small = gpu_project(pkg, torch_cuda, config, records,
+                        tuning=pkg.TuningParameters(track_tile_size=256))
+    assert np.array_equal(got[0], small[0]) and np.array_equal(got[1], small[1])
+    assert got[2]["fixed_point_overflows"] == 0
+    assert max(np.abs(got[0]).max(), np.abs(got[1]).max()) > 2 ** 61
+    if precision == 0:
+        want = oracle.restatement().project(config, records, threads=8)
+        assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
+
+
 def test_empty_and_repeated_batches(pkg, oracle, showers, torch_cuda):
     wl, records = _workload_records(showers, "plain_c0", 40_000, seed=4)
     config = showers.make_config(wl, kernel=2)
