@@ -202,7 +202,7 @@ class Accumulator {
     precision_ = config.precision == C8R_PRECISION_MIXED ? Precision::kMixed : Precision::kFP64;
     kernel_ = config.kernel;
     host_batch_ = tuning.batch_size ? static_cast<std::size_t>(tuning.batch_size) : kDefaultHostBatch;
-    threads_ = tuning.team_size ? static_cast<int>(tuning.team_size) : 512;
+    threads_ = tuning.team_size ? static_cast<int>(tuning.team_size) : kWindowThreads;
     upload_static();
     allocate_traces();
     counters_.allocate(1);
@@ -416,7 +416,7 @@ class Accumulator {
   void set_tuning(c8r_tuning const& t) {
     if (t.team_size > static_cast<uint64_t>(kWindowThreads) || (t.team_size != 0 && t.team_size % 32 != 0))
       throw std::invalid_argument("radio tuning is invalid");
-    threads_ = t.team_size ? static_cast<int>(t.team_size) : 512;
+    threads_ = t.team_size ? static_cast<int>(t.team_size) : kWindowThreads;
     tuning_.team_size = t.team_size;
     tuning_.track_tile_size = t.track_tile_size;
     stats_.track_tile_size = static_cast<uint32_t>(t.track_tile_size);
@@ -925,7 +925,7 @@ class Batch {
   // Sweeps block size x chunk size (tracks per work item) on the staged
   // events, keeps the fastest, and zeroes the traces it wrote.
   c8r_tuning autotune(Accumulator* const* events, std::size_t n, int repetitions, double& best_ms) {
-    static constexpr uint64_t kTeams[] = {256, 384, 512};
+    static constexpr uint64_t kTeams[] = {256, 384, 512, 640};
     static constexpr uint64_t kChunks[] = {0, 32768, 131072, 524288};
     c8r_tuning best{};
     best_ms = -1.;

@@ -768,6 +768,12 @@ __device__ __forceinline__ void deposit_staged(StagedSegment<Amp>* staging,
   staging[lane] = seg;
   __syncwarp();
   uint32_t const before_mine = incl - cnt;
+  // the converting fields in registers: `o` lives in shared memory, which the
+  // window atomics below might alias as far as the compiler can tell
+  ObserverCache grid;
+  grid.fixed_scale = o.fixed_scale;
+  grid.fixed_scale_f = o.fixed_scale_f;
+  grid.count_samples = o.count_samples;
   for (uint32_t base = 0; base < total; base += 32u) {
     uint32_t const j = base + lane;
     uint32_t owner = 0;
@@ -789,7 +795,7 @@ __device__ __forceinline__ void deposit_staged(StagedSegment<Amp>* staging,
         bin = g.last_bin;
         scale = g.last;
       }
-      deposit_bin<kFixed>(sink, bin, make_deposit<kFixed>(o, scaled(g.perp, scale)), c.zhs,
+      deposit_bin<kFixed>(sink, bin, make_deposit<kFixed>(grid, scaled(g.perp, scale)), c.zhs,
                           c.overflows, c.mag);
     }
   }
@@ -1148,7 +1154,7 @@ __global__ void __launch_bounds__(256) direct_kernel(const __grid_constant__ Eve
 }
 
 // ---------------------------------------------------------------- windowed
-constexpr int kWindowThreadsMax = 512;
+constexpr int kWindowThreadsMax = kWindowThreads;
 // The ZHS kernel's live state needs more than 128 registers a thread: it runs
 // 384-thread CTAs (up to 168 registers, no spills).
 constexpr int kZhsThreadsMax = 384;

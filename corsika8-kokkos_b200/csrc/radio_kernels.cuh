@@ -62,7 +62,7 @@ struct EventPlan {
 // observer) items drawn from an atomic counter.  Passed as a __grid_constant__
 // kernel parameter (no host-to-device copy; graph-capturable).
 constexpr int kMaxEventsPerLaunch = 64;
-constexpr int kWindowThreads = 512;  // upper bound of the windowed block size
+constexpr int kWindowThreads = 640;  // upper bound (and default) of the windowed block size
 struct WorkPlan {
   EventPlan events[kMaxEventsPerLaunch];
   int32_t algorithm;        // 0: CoREAS items, 1: ZHS items

@@ -190,12 +190,12 @@ class Server {
     block_tracks_ = options.block_tracks ? options.block_tracks : (1u << 20);
     chunk_tracks_ = options.chunk_tracks ? options.chunk_tracks : 16384;
     round_pairs_ = options.round_pairs ? options.round_pairs : 400000000ull;
-    threads_ = options.team_size ? static_cast<int>(options.team_size) : 512;
+    threads_ = options.team_size ? static_cast<int>(options.team_size) : kWindowThreads;
     if (chunk_tracks_ == 0 || chunk_tracks_ > 0x7fffffffu || block_tracks_ % chunk_tracks_ != 0 ||
         block_tracks_ / chunk_tracks_ > 0xffffffffu)
       throw std::invalid_argument("server block_tracks must be a multiple of chunk_tracks");
     if (threads_ > kWindowThreads || threads_ % 32 != 0 || threads_ < 32)
-      throw std::invalid_argument("server team_size must be a multiple of 32 up to 512");
+      throw std::invalid_argument("server team_size must be a multiple of 32 up to 640");
     check(cudaGetDevice(&device_), "cudaGetDevice");
     check(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, device_), "SM count");
     max_window_ = windowed_max_bins(device_);
@@ -761,7 +761,7 @@ class Server {
     ++stats_.rounds;
   }
 
-  int device_ = 0, sms_ = 148, threads_ = 512, max_window_ = 0;
+  int device_ = 0, sms_ = 148, threads_ = kWindowThreads, max_window_ = 0;
   uint64_t block_tracks_ = 0, chunk_tracks_ = 0, round_pairs_ = 0;
   std::size_t block_bytes_ = 0;
   Arena arena_;

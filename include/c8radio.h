@@ -306,7 +306,7 @@ int c8r_batch_create(void* stream, c8r_batch** batch);
 void c8r_batch_destroy(c8r_batch* batch);
 const char* c8r_batch_last_error(const c8r_batch* batch);
 int c8r_batch_project(c8r_batch* batch, c8r_accumulator* const* events, size_t count, int flags);
-/* Sweeps team size {256,384,512} x tracks per item {auto,32768,131072,524288}
+/* Sweeps team size {256,384,512,640} x tracks per item {auto,32768,131072,524288}
  * on the staged events (repetitions timed runs each), applies the fastest to
  * every event, zeroes the traces the sweep wrote and returns it. */
 int c8r_batch_autotune(c8r_batch* batch, c8r_accumulator* const* events, size_t count,
@@ -332,7 +332,7 @@ typedef struct c8r_server_options {
   uint64_t block_tracks; /* tracks per kinematics block; 0 = 1048576 */
   uint64_t chunk_tracks; /* tracks per work item; 0 = 16384 (divides block_tracks) */
   uint64_t round_pairs;  /* track-antenna pairs per round; 0 = 4e8 */
-  uint32_t team_size;    /* threads per windowed CTA; 0 = 512 */
+  uint32_t team_size;    /* threads per windowed CTA; 0 = 640 (ZHS launches at most 384) */
   uint32_t reserved_[7];
 } c8r_server_options;
 typedef struct c8r_server_event_info {
