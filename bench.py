@@ -69,6 +69,8 @@ def parse_args():
     p.add_argument("--serve-budget-gb", type=float, default=120.0)
     p.add_argument("--library-segments", type=int, default=500_000,
                    help="segments of each of the 15 replayed library showers")
+    p.add_argument("--precision-study", action="store_true",
+                   help="print the arrival-time precision study of the ice workload instead")
     p.add_argument("--plain-fraction", type=int, default=8,
                    help="the plain event-by-event comparison projects 1/N of every event's segments")
     return p.parse_args()
@@ -502,6 +504,78 @@ def run_serving(pkg, showers, torch, args, local: int) -> dict:
     }
 
 
+# ------------------------------------------------------------------ precision study
+STUDY_MODES = (("fp64", 0, 2), ("mixed", 1, 2), ("study_fp64", 4, 0), ("double_fp32", 2, 0),
+               ("fp32", 3, 0))
+
+
+def run_precision_study(args):
+    """The ice workload (uniform n = 1.78, antennas on and +-0.5 deg around the
+    Cherenkov cone) with its arrival times, distances, directions and Cherenkov
+    denominators in FP64 (the reference's arithmetic), the mixed production
+    path, and the generic study kernel in FP64, compensated double-FP32 and
+    FP32.  Per mode: samples whose bin differs from FP64 (from sample-count
+    traces), per-trace relative L2 and peak-amplitude error of the decoded
+    traces against FP64, and pairs/s."""
+    import torch
+
+    pkg, showers, wl, records = build_workload("ice_c2", args.segments, seed=2000)
+    raw = torch.from_numpy(records.view(np.uint8).reshape(-1)).cuda()
+    observers = wl["observers"]
+    bins = int(observers["number_of_bins"][0])
+    pairs = records.size * len(observers)
+
+    def project(precision, kernel, count_samples, timed=False):
+        config = showers.make_config(wl, precision=precision, kernel=kernel, count_samples=count_samples)
+        acc = pkg.RadioAccumulator(config)
+        if timed:
+            acc.accumulate_lepton_tracks(raw.data_ptr(), records.size)
+            acc.reset()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        acc.accumulate_lepton_tracks(raw.data_ptr(), records.size)
+        torch.cuda.synchronize()
+        seconds = time.perf_counter() - t0
+        out = acc.download_fixed() if count_samples else acc.download()
+        acc.close()
+        return out, seconds
+
+    reference_counts = None
+    reference = None
+    rows = {}
+    for name, precision, kernel in STUDY_MODES:
+        (counts_c, counts_z, counters), _ = project(precision, kernel, True)
+        waveforms, seconds = project(precision, kernel, False, timed=True)
+        if reference_counts is None:
+            reference_counts = (counts_c, counts_z, counters)
+            reference = waveforms
+        row = {"pairs_per_s": pairs / seconds, "kernel": "windowed" if kernel == 2 else "study"}
+        for label, got, want, key in (("coreas", counts_c, reference_counts[0], "coreas_contributions"),
+                                      ("zhs", counts_z, reference_counts[1], "zhs_contributions")):
+            moved = int(np.abs(got[0] - want[0]).sum()) // 2 + abs(int(got[0].sum()) - int(want[0].sum())) // 2
+            row[f"{label}_samples"] = int(counters[key])
+            row[f"{label}_samples_in_other_bins"] = moved
+            row[f"{label}_bin_agreement"] = 1.0 - moved / max(int(want[0].sum()), 1)
+        for label, got, want in (("coreas", waveforms.coreas, reference.coreas),
+                                 ("zhs", waveforms.zhs, reference.zhs)):
+            g = got.reshape(3, -1, bins)
+            w = want.reshape(3, -1, bins)
+            norm = np.sqrt((w ** 2).sum(axis=(0, 2)))
+            ok = norm > 0
+            rel = np.sqrt(((g - w) ** 2).sum(axis=(0, 2)))[ok] / norm[ok]
+            gp = np.abs(g).max(axis=(0, 2))[ok]
+            wp = np.abs(w).max(axis=(0, 2))[ok]
+            row[f"{label}_max_rel_l2"] = float(rel.max()) if rel.size else 0.0
+            row[f"{label}_median_rel_l2"] = float(np.median(rel)) if rel.size else 0.0
+            row[f"{label}_max_peak_error"] = float((np.abs(gp - wp) / wp).max()) if rel.size else 0.0
+        rows[name] = row
+        print(f"# {name}: {json.dumps(row)}", file=sys.stderr, flush=True)
+    print(json.dumps({"study": "arrival-time precision", "workload": "ice_c2",
+                      "segments": int(records.size), "antennas": int(len(observers)), "bins": bins,
+                      "pairs": pairs, "reference_mode": "fp64 (windowed, the reference's arithmetic)",
+                      "modes": rows}), flush=True)
+
+
 def run_e2e(pkg, showers, wl, records, precision, kernel, stream, args, torch, barrier,
             max_over_ranks, world):
     """reset + enqueueHostLeptonTracks(pinned host records) + download(pinned traces)."""
@@ -537,7 +611,9 @@ def run_e2e(pkg, showers, wl, records, precision, kernel, stream, args, torch, b
 
 def main():
     args = parse_args()
-    if args.impl == "reference":
+    if args.precision_study:
+        run_precision_study(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

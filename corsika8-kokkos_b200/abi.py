@@ -69,6 +69,9 @@ C8R_TIMEOUT = 9
 
 PRECISION_FP64 = 0
 PRECISION_MIXED = 1
+PRECISION_STUDY_DOUBLE_FP32 = 2
+PRECISION_STUDY_FP32 = 3
+PRECISION_STUDY_FP64 = 4
 KERNEL_AUTO = 0
 KERNEL_DIRECT = 1
 KERNEL_WINDOWED = 2

@@ -123,7 +123,7 @@ void validate(c8r_config const& config) {
        !(p.step_m > 0.) || !std::isfinite(p.inverse_step_per_m) ||
        !(p.inverse_step_per_m > 0.)))
     throw std::invalid_argument("invalid flat-atmosphere radio snapshot");
-  if (config.precision != C8R_PRECISION_FP64 && config.precision != C8R_PRECISION_MIXED)
+  if (config.precision < C8R_PRECISION_FP64 || config.precision > C8R_PRECISION_STUDY_FP64)
     throw std::invalid_argument("invalid radio precision");
   if (config.kernel < C8R_KERNEL_AUTO || config.kernel > C8R_KERNEL_WINDOWED)
     throw std::invalid_argument("invalid radio kernel selection");
@@ -200,6 +200,9 @@ class Accumulator {
     copy_config(config);
     fixed_ = config.deterministic != 0;
     precision_ = config.precision == C8R_PRECISION_MIXED ? Precision::kMixed : Precision::kFP64;
+    study_ = config.precision >= C8R_PRECISION_STUDY_DOUBLE_FP32;
+    if (config.precision == C8R_PRECISION_STUDY_DOUBLE_FP32) arithmetic_ = TimeArithmetic::kDoubleFloat;
+    if (config.precision == C8R_PRECISION_STUDY_FP32) arithmetic_ = TimeArithmetic::kFloat;
     kernel_ = config.kernel;
     host_batch_ = tuning.batch_size ? static_cast<std::size_t>(tuning.batch_size) : kDefaultHostBatch;
     threads_ = tuning.team_size ? static_cast<int>(tuning.team_size) : kWindowThreads;
@@ -382,7 +385,9 @@ class Accumulator {
     }
     bool const direct = kernel_ == C8R_KERNEL_DIRECT ||
                         (kernel_ == C8R_KERNEL_AUTO && count < kDirectThreshold);
-    if (direct)
+    if (study_)
+      project_study(count);
+    else if (direct)
       project_direct(count);
     else
       project_windowed(count);
@@ -575,6 +580,7 @@ class Accumulator {
   EventPlan event_plan(std::size_t count) const { return make_event(count); }
   bool fixed() const { return fixed_; }
   Precision precision() const { return precision_; }
+  bool study() const { return study_; }
   int sms() const { return sms_; }
   int threads() const { return threads_; }
   uint32_t window_bins() const { return static_cast<uint32_t>(window_bins_); }
@@ -766,6 +772,16 @@ class Accumulator {
     stats_.direct_projection_records += count;
   }
 
+  // The precision study's generic kernel, both algorithms in one launch.
+  void project_study(std::size_t count) {
+    EventPlan const ev = make_event(count);
+    bool const c = ev.observer_count[0] != 0, z = ev.observer_count[1] != 0;
+    check(launch_study(ev, count, c, z, fixed_, arithmetic_, stream_), "study launch");
+    stats_.track_observer_pairs += count * (ev.observer_count[0] + ev.observer_count[1]);
+    ++stats_.direct_projection_batches;
+    stats_.direct_projection_records += count;
+  }
+
   // One persistent launch per algorithm (CoREAS items, then ZHS items): each
   // kernel instance carries one algorithm's code only.
   void project_windowed(std::size_t count) {
@@ -829,6 +845,8 @@ class Accumulator {
   bool downloaded_ = false, sealed_ = false, timing_ = false;
   int kernel_ = C8R_KERNEL_AUTO;
   Precision precision_ = Precision::kFP64;
+  bool study_ = false;
+  TimeArithmetic arithmetic_ = TimeArithmetic::kDouble;
   double limit_ = 1.;
   c8r_tuning tuning_{};
   Propagation propagation_{};
@@ -994,6 +1012,7 @@ class Batch {
       if (!e->enabled() || e->staged() == 0) continue;
       if (e->sealed()) throw std::logic_error("radio endpoint already committed; reset before new tracks");
       if (e->stream() != stream_) throw std::invalid_argument("batched accumulators must share the batch stream");
+      if (e->study()) throw std::invalid_argument("precision-study accumulators cannot be batched");
       EventPlan ev = e->event_plan(e->staged());
       if (active.empty()) {
         fixed = e->fixed();

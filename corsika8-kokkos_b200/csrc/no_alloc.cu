@@ -141,6 +141,8 @@ void accumulate_no_alloc(c8r_config const& config, c8r_lepton_transport_record c
   if (c8r_config_validate(&config) != C8R_OK) throw std::invalid_argument(c8r_last_global_error());
   if (count > extent) throw std::out_of_range("radio track count exceeds input view");
   if (count != 0 && records == nullptr) throw std::invalid_argument("null device radio track input");
+  if (config.precision > C8R_PRECISION_MIXED)
+    throw std::invalid_argument("no-alloc radio call takes FP64 or mixed precision");
   bool const on[2] = {config.coreas_enabled != 0, config.zhs_enabled != 0};
   std::size_t const observers[2] = {on[0] ? config.coreas_observer_count : 0,
                                     on[1] ? config.zhs_observer_count : 0};

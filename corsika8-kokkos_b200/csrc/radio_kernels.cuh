@@ -95,6 +95,13 @@ int windowed_max_bins(int device);
 // Resident CTAs per SM of the windowed kernel for a window and block size.
 int windowed_ctas_per_sm(int window, int threads, bool fixed, Precision precision);
 
+// The precision study's kernel (precision_study.cu): one thread per pair,
+// arrival-time arithmetic in FP64, compensated double-FP32 or FP32,
+// amplitudes in FP32.
+enum class TimeArithmetic : int { kDouble = 0, kDoubleFloat = 1, kFloat = 2 };
+cudaError_t launch_study(EventPlan const& event, uint64_t track_bound, bool coreas, bool zhs,
+                         bool fixed, TimeArithmetic arithmetic, cudaStream_t stream);
+
 // Fixed-point decode on the device: out[r*bins + i] = in[r*bins + i] * factor(observer).
 cudaError_t launch_decode(const long long* fixed, double* out, uint64_t total_bins,
                           const uint64_t* observer_offsets, const double* factors,

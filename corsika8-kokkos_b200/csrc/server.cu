@@ -243,6 +243,8 @@ class Server {
     double const opened = now();
     if (!config.enabled) throw std::invalid_argument("served radio event must be enabled");
     if (c8r_config_validate(&config) != C8R_OK) throw std::invalid_argument(c8r_last_global_error());
+    if (config.precision > C8R_PRECISION_MIXED)
+      throw std::invalid_argument("served radio events take FP64 or mixed precision");
     auto ev = std::make_unique<ServedEvent>();
     ev->open_s = opened;
     ev->fixed = config.deterministic != 0;

@@ -96,9 +96,14 @@ typedef struct c8r_propagation_snapshot {
 enum {
   C8R_PRECISION_FP64 = 0,  /* every expression in FP64, operation for operation as
                               the reference: the plain drop-in */
-  C8R_PRECISION_MIXED = 1  /* arrival times, distances, emission directions and
+  C8R_PRECISION_MIXED = 1, /* arrival times, distances, emission directions and
                               1 - n beta.k in FP64 (bin indices and branches are
                               identical); field and potential amplitudes in FP32 */
+  /* Precision study (one thread per pair, accumulate and download only): the
+     arrival-time, distance, direction and 1 - n beta.k arithmetic in ... */
+  C8R_PRECISION_STUDY_DOUBLE_FP32 = 2, /* compensated double-FP32 (hi + lo floats) */
+  C8R_PRECISION_STUDY_FP32 = 3,        /* plain FP32 (bins may differ) */
+  C8R_PRECISION_STUDY_FP64 = 4         /* FP64 through the same generic kernel (its check) */
 };
 
 /* Kernel family used by accumulate. */
