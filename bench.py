@@ -69,6 +69,9 @@ def parse_args():
     p.add_argument("--serve-budget-gb", type=float, default=120.0)
     p.add_argument("--library-segments", type=int, default=500_000,
                    help="segments of each of the 15 replayed library showers")
+    p.add_argument("--batched", action="store_true",
+                   help="print the batched workload (64 events, one graph-replayed launch per algorithm) instead")
+    p.add_argument("--batch-events", type=int, default=64)
     p.add_argument("--precision-study", action="store_true",
                    help="print the arrival-time precision study of the ice workload instead")
     p.add_argument("--plain-fraction", type=int, default=8,
@@ -504,6 +507,71 @@ def run_serving(pkg, showers, torch, args, local: int) -> dict:
     }
 
 
+# ------------------------------------------------------------------ batched
+def run_batched(args):
+    """Batched workload: `batch_events` events (segments log-uniform 1e5-2e7,
+    16-300 antennas, zenith 0-60 deg, Xmax 550-850 g/cm^2, 4096 bins), each
+    staged into its own accumulator (mixed precision) from a device-resident
+    library of seeded showers, then projected together by one persistent launch
+    per algorithm, replayed from a captured CUDA graph.  The tile shape (threads
+    per CTA x tracks per work item) is chosen first by the autotuner on the
+    first eighth of the events.  Timed: K graph replays, CUDA events."""
+    import torch
+
+    pkg = entry.load_package()
+    from corsika8_kokkos_b200 import showers
+
+    specs = showers.batched_event_specs(events=args.batch_events)
+    size = args.library_segments
+    library = showers.shower_library(size)
+    itemsize = next(iter(library.values())).itemsize
+    dev = {k: torch.from_numpy(v.view(np.uint8).reshape(-1)).cuda() for k, v in library.items()}
+    stream = torch.cuda.Stream()
+    events = []
+    for spec in specs:
+        wl, _ = showers.event_workload(spec)
+        acc = pkg.RadioAccumulator(showers.make_config(wl, precision=1, kernel=2),
+                                   stream=stream.cuda_stream)
+        acc.reserve_track_capacity(spec.segments)
+        base = dev[showers.library_key(spec)].data_ptr()
+        for offset, n in showers.replay_slices(spec.segments, size):
+            acc.stage_lepton_tracks(base + offset * itemsize, n)
+        events.append(acc)
+    stream.synchronize()
+    pairs = sum(s.segments * s.antennas for s in specs)
+    batch = pkg.RadioBatch(stream=stream.cuda_stream)
+    tune = events[: max(1, len(events) // 8)]
+    best, best_ms = batch.autotune(tune, repetitions=1)
+    for acc in events:
+        acc.set_tuning(best)
+    for _ in range(max(1, args.warmup)):
+        batch.project(events, graph=True, keep_staged=True)
+    stream.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(0) as clocks:
+        start.record(stream)
+        for _ in range(args.steps):
+            batch.project(events, graph=True, keep_staged=True)
+        end.record(stream)
+        stream.synchronize()
+    ms = start.elapsed_time(end) / args.steps
+    captures = batch.graph_captures()
+    batch.close()
+    for acc in events:
+        acc.close()
+    print(json.dumps({
+        "metric": "track-antenna pairs/s", "value": pairs / (ms * 1e-3), "unit": "pairs/s",
+        "workload": f"batched_c3: {len(specs)} events, segments log-uniform 1e5-2e7, 16-300 antennas, "
+                    f"zenith 0-60, Xmax 550-850, 4096 bins, CoREAS+ZHS, mixed precision, fixed point",
+        "inputs": f"device-resident replay of 15 seeded library showers ({size} segments each), staged",
+        "events": len(specs), "segments": int(sum(s.segments for s in specs)), "pairs_per_step": int(pairs),
+        "steps": args.steps, "ms_per_step": ms, "launches_per_step": 2, "graph_captures": int(captures),
+        "autotune": {"team_size": best.team_size, "track_tile_size": best.track_tile_size,
+                     "ms": best_ms, "events": len(tune)},
+        "clocks": clocks.summary(),
+    }), flush=True)
+
+
 # ------------------------------------------------------------------ precision study
 STUDY_MODES = (("fp64", 0, 2), ("mixed", 1, 2), ("study_fp64", 4, 0), ("double_fp32", 2, 0),
                ("fp32", 3, 0))
@@ -613,6 +681,8 @@ def main():
     args = parse_args()
     if args.precision_study:
         run_precision_study(args)
+    elif args.batched:
+        run_batched(args)
     elif args.impl == "reference":
         run_reference(args)
     else:
