@@ -510,3 +510,104 @@ class RadioServer:
 
     def __exit__(self, *exc):
         self.close()
+
+
+# ------------------------------------------------------------------ spool
+class SpoolWriter:
+    """RadioTrackSpoolWriter (version 1): refuses an existing path; tracks are
+    validated on append; only complete() publishes the record count."""
+
+    def __init__(self, path):
+        self._lib = library()
+        handle = C.c_void_p()
+        _raise(self._lib.c8r_spool_writer_create(str(path).encode(), C.byref(handle)),
+               self._lib.c8r_last_global_error())
+        self._h = handle
+
+    def append(self, tracks: np.ndarray) -> None:
+        tracks = np.ascontiguousarray(tracks, dtype=abi.TRACK_SEGMENT)
+        _raise(self._lib.c8r_spool_append(self._h, tracks.ctypes.data if tracks.size else None,
+                                          tracks.size), self._lib.c8r_last_global_error())
+
+    def complete(self) -> None:
+        _raise(self._lib.c8r_spool_complete(self._h), self._lib.c8r_last_global_error())
+
+    def count(self) -> int:
+        out = C.c_uint64()
+        _raise(self._lib.c8r_spool_writer_count(self._h, C.byref(out)), self._lib.c8r_last_global_error())
+        return out.value
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.c8r_spool_writer_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class SpoolReader:
+    """RadioTrackSpoolReader (version 1): validates the header and file length
+    on open; read_batch returns at most `maximum` (1..65536) validated tracks."""
+
+    def __init__(self, path):
+        self._lib = library()
+        handle, count = C.c_void_p(), C.c_uint64()
+        _raise(self._lib.c8r_spool_reader_open(str(path).encode(), C.byref(handle), C.byref(count)),
+               self._lib.c8r_last_global_error())
+        self._h = handle
+        self.count = count.value
+
+    def read_batch(self, maximum: int = 4096) -> np.ndarray:
+        out = np.zeros(max(int(maximum), 0), abi.TRACK_SEGMENT)
+        n = C.c_size_t()
+        _raise(self._lib.c8r_spool_read(self._h, out.ctypes.data if out.size else None, int(maximum),
+                                        C.byref(n)), self._lib.c8r_last_global_error())
+        return out[: n.value]
+
+    def state(self):
+        consumed, finished = C.c_uint64(), C.c_int()
+        _raise(self._lib.c8r_spool_reader_state(self._h, C.byref(consumed), C.byref(finished)),
+               self._lib.c8r_last_global_error())
+        return consumed.value, bool(finished.value)
+
+    def replay(self, accumulator: "RadioAccumulator", batch: int = 4096) -> None:
+        """Enqueues every remaining track into the accumulator as host tracks."""
+        _raise(self._lib.c8r_spool_replay(self._h, accumulator._h, int(batch)),
+               self._lib.c8r_last_global_error())
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.c8r_spool_reader_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def track_records(tracks: np.ndarray) -> np.ndarray:
+    """make_host_radio_record for each track segment (LeptonTransportRecords)."""
+    lib = library()
+    tracks = np.ascontiguousarray(tracks, dtype=abi.TRACK_SEGMENT)
+    out = np.zeros(tracks.size, LEPTON_RECORD)
+    _raise(lib.c8r_track_records(tracks.ctypes.data if tracks.size else None, tracks.size,
+                                 out.ctypes.data if out.size else None), lib.c8r_last_global_error())
+    return out

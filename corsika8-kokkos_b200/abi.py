@@ -213,6 +213,14 @@ class Peaks(C.Structure):
 
 
 # Exported symbols of libc8radio.so and their prototypes.
+TRACK_SEGMENT = np.dtype([
+    ("pdg", np.int32), ("start_position_m", np.float64, 3), ("end_position_m", np.float64, 3),
+    ("start_direction", np.float64, 3), ("end_direction", np.float64, 3), ("start_time_s", np.float64),
+    ("end_time_s", np.float64), ("start_kinetic_energy_gev", np.float64),
+    ("end_kinetic_energy_gev", np.float64), ("weight", np.float64)], align=True)
+assert TRACK_SEGMENT.itemsize == 144
+
+
 class ServerOptions(C.Structure):
     _fields_ = [
         ("budget_bytes", C.c_uint64),
@@ -297,6 +305,17 @@ PROTOTYPES = {
     "c8r_server_fetch": (C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p,
                                    C.POINTER(Counters), C.POINTER(ServerEventInfo)]),
     "c8r_server_get_stats": (C.c_int, [C.c_void_p, C.POINTER(ServerStats)]),
+    "c8r_spool_writer_create": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
+    "c8r_spool_append": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t]),
+    "c8r_spool_complete": (C.c_int, [C.c_void_p]),
+    "c8r_spool_writer_count": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
+    "c8r_spool_writer_destroy": (None, [C.c_void_p]),
+    "c8r_spool_reader_open": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p), C.POINTER(C.c_uint64)]),
+    "c8r_spool_read": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)]),
+    "c8r_spool_reader_state": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_int)]),
+    "c8r_spool_reader_destroy": (None, [C.c_void_p]),
+    "c8r_track_records": (C.c_int, [C.c_void_p, C.c_size_t, C.c_void_p]),
+    "c8r_spool_replay": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t]),
     "c8r_accumulate_device_no_alloc": (C.c_int, [C.POINTER(Config), C.c_void_p, C.c_size_t, C.c_size_t,
                                                  C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
 }

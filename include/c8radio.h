@@ -318,6 +318,47 @@ int c8r_batch_autotune(c8r_batch* batch, c8r_accumulator* const* events, size_t 
                        int repetitions, c8r_tuning* best, double* best_ms);
 int c8r_batch_graph_captures(const c8r_batch* batch, unsigned long long* captures);
 
+/* ---- Track spool, version 1: completed host tracks on disk ----------------
+ * corsika/kokkos/radio/RadioTrackSpoolFormat.hpp:24-29 and
+ * RadioTrackSpool{Reader,Writer}.hpp: a 32-byte header ("C8_RADIO_TRACKS\0",
+ * version 1, record size 140, record count, all ones until completed) and
+ * one 140-byte little-endian record per track.  Failures return
+ * C8R_RUNTIME_ERROR with c8r_last_global_error() set, as the reference throws
+ * std::runtime_error. */
+typedef struct c8r_track_segment { /* corsika::radio::RadioTrackSegment */
+  int32_t pdg;                     /* 11 or -11 */
+  double start_position_m[3];
+  double end_position_m[3];
+  double start_direction[3];
+  double end_direction[3];
+  double start_time_s;
+  double end_time_s;
+  double start_kinetic_energy_gev;
+  double end_kinetic_energy_gev;
+  double weight;
+} c8r_track_segment;
+typedef struct c8r_spool_writer c8r_spool_writer;
+typedef struct c8r_spool_reader c8r_spool_reader;
+/* RadioTrackSpoolWriter (RadioTrackSpoolWriter.inl:11-45): refuses an existing
+ * path; append validates each track; only complete() publishes the count. */
+int c8r_spool_writer_create(const char* path, c8r_spool_writer** writer);
+int c8r_spool_append(c8r_spool_writer* writer, const c8r_track_segment* tracks, size_t count);
+int c8r_spool_complete(c8r_spool_writer* writer);
+int c8r_spool_writer_count(const c8r_spool_writer* writer, uint64_t* count);
+void c8r_spool_writer_destroy(c8r_spool_writer* writer);
+/* RadioTrackSpoolReader (RadioTrackSpoolReader.inl:11-47): validates magic,
+ * version, record size, completion and file length; reads at most `maximum`
+ * (1..65536) tracks per call, each validated. */
+int c8r_spool_reader_open(const char* path, c8r_spool_reader** reader, uint64_t* count);
+int c8r_spool_read(c8r_spool_reader* reader, c8r_track_segment* tracks, size_t maximum, size_t* read);
+int c8r_spool_reader_state(const c8r_spool_reader* reader, uint64_t* consumed, int* finished);
+void c8r_spool_reader_destroy(c8r_spool_reader* reader);
+/* make_host_radio_record (HostRadioRecord.inl:11-31): total energy = kinetic + m_e. */
+int c8r_track_records(const c8r_track_segment* tracks, size_t count, c8r_lepton_transport_record* records);
+/* Replays every remaining track of a spool into an accumulator as host tracks
+ * (c8r_enqueue_host), read in batches of `batch` (1..65536). */
+int c8r_spool_replay(c8r_spool_reader* reader, c8r_accumulator* accumulator, size_t batch);
+
 /* ---- Serving: many showers in flight on one GPU ---------------------------
  * No reference counterpart (the reference runs one shower per accumulator).
  * A server reserves one HBM arena of budget_bytes at creation and admits
