@@ -356,6 +356,15 @@ class RadioAccumulator:
     def set_kernel_timing(self, enabled: bool) -> None:
         self._check(self._lib.c8r_set_kernel_timing(self._h, int(enabled)))
 
+    def download_fields_device(self, coreas_pointer: Optional[int], zhs_pointer: Optional[int]) -> dict:
+        """Adds the decoded CoREAS fields (3 x coreas_bins doubles) and the ZHS
+        fields -(A[i+1] - A[i]) fs (3 x (zhs_bins - zhs observers) doubles) into
+        device buffers; returns the counters.  Seals the accumulator."""
+        counters = abi.Counters()
+        self._check(self._lib.c8r_download_fields_device(
+            self._h, C.c_void_p(coreas_pointer or 0), C.c_void_p(zhs_pointer or 0), C.byref(counters)))
+        return counters.as_dict()
+
     # B200 extensions: staging for batched projection -----------------------
     def stage_lepton_tracks(self, device_pointer: int, count: int,
                             extent: Optional[int] = None) -> None:
@@ -611,3 +620,16 @@ def track_records(tracks: np.ndarray) -> np.ndarray:
     _raise(lib.c8r_track_records(tracks.ctypes.data if tracks.size else None, tracks.size,
                                  out.ctypes.data if out.size else None), lib.c8r_last_global_error())
     return out
+
+
+def merge_fixed(destination: np.ndarray, source: np.ndarray) -> None:
+    """destination += source for int64 fixed-point snapshots, every bin checked
+    first (OverflowErrorRadio, nothing written, on overflow)."""
+    lib = library()
+    if destination.dtype != np.int64 or source.dtype != np.int64 or destination.shape != source.shape:
+        raise InvalidArgument("merge_fixed takes two int64 arrays of one shape")
+    if not destination.flags["C_CONTIGUOUS"]:
+        raise InvalidArgument("merge_fixed destination must be contiguous")
+    source = np.ascontiguousarray(source)
+    _raise(lib.c8r_merge_fixed(destination.ctypes.data, source.ctypes.data, destination.size),
+           lib.c8r_last_global_error())

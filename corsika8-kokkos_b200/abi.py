@@ -305,6 +305,8 @@ PROTOTYPES = {
     "c8r_server_fetch": (C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p,
                                    C.POINTER(Counters), C.POINTER(ServerEventInfo)]),
     "c8r_server_get_stats": (C.c_int, [C.c_void_p, C.POINTER(ServerStats)]),
+    "c8r_download_fields_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(Counters)]),
+    "c8r_merge_fixed": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t]),
     "c8r_spool_writer_create": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
     "c8r_spool_append": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t]),
     "c8r_spool_complete": (C.c_int, [C.c_void_p]),

@@ -500,6 +500,37 @@ class Accumulator {
     downloaded_ = true;
   }
 
+  // The output step on the device (RadioProcess.inl:213-223 and the observer
+  // add of CorsikaOutputSink.inl:255-278): decoded CoREAS fields and
+  // differentiated ZHS fields added into caller-owned device buffers, with
+  // download()'s checks and sealing.
+  void download_fields_device(double* coreas, double* zhs, c8r_counters* counters) {
+    if (!enabled()) {
+      if (counters) *counters = c8r_counters{};
+      return;
+    }
+    if (downloaded_ || sealed_) throw std::logic_error("radio waveforms downloaded twice");
+    flush();
+    project_staged(true);
+    DeviceCounters host{};
+    fetch_counters(host);
+    if (host.fixed_point_overflows != 0)
+      throw std::runtime_error(
+          "radio fixed-point accumulator overflowed; increase fixed_point_field_limit_V_per_m");
+    for (int a = 0; a < 2; ++a) {
+      double* out = a == 0 ? coreas : zhs;
+      if (out == nullptr || bins_[a] == 0 || observers_host_[a].empty()) continue;
+      check(launch_output(fixed_ ? reinterpret_cast<long long const*>(fixed_traces_[a].ptr) : nullptr,
+                          float_traces_[a].ptr, out, bins_[a], observers_[a].ptr, decode_factors_[a].ptr,
+                          static_cast<uint32_t>(observers_host_[a].size()), max_observer_bins_[a], a == 1,
+                          stream_),
+            "output launch");
+    }
+    check(cudaStreamSynchronize(stream_), "output fence");
+    if (counters) std::memcpy(counters, &host, sizeof(host));
+    downloaded_ = true;
+  }
+
   // RadioAccumulator::downloadFixed, RadioAccumulator.inl:359-405: raw int64.
   void download_fixed(long long* coreas, long long* zhs, c8r_counters* counters) {
     if (!enabled() || !fixed_ || downloaded_ || sealed_)
@@ -1234,6 +1265,28 @@ int c8r_download_fixed(c8r_accumulator* handle, long long* coreas_xyz, long long
   if (int s = with_handle(handle, nullptr, true)) return s;
   return guarded(&handle->error,
                  [&] { handle->impl->download_fixed(coreas_xyz, zhs_xyz, counters); });
+}
+
+int c8r_download_fields_device(c8r_accumulator* handle, double* coreas_field_xyz, double* zhs_field_xyz,
+                               c8r_counters* counters) {
+  if (int s = with_handle(handle, nullptr, true)) return s;
+  return guarded(&handle->error,
+                 [&] { handle->impl->download_fields_device(coreas_field_xyz, zhs_field_xyz, counters); });
+}
+
+// merge_fixed_accumulators (FixedAccumulatorMerge.inl:12-29) without the layout
+// labels: every bin checked before any is written.
+int c8r_merge_fixed(long long* destination, const long long* source, size_t count) {
+  return guarded(&g_last_error, [&] {
+    if (count && (!destination || !source)) throw std::invalid_argument("null argument");
+    for (size_t i = 0; i < count; ++i) {
+      long long const x = destination[i], y = source[i];
+      if ((y > 0 && x > std::numeric_limits<long long>::max() - y) ||
+          (y < 0 && x < std::numeric_limits<long long>::min() - y))
+        throw std::overflow_error("cooperative fixed-point accumulation overflow");
+    }
+    for (size_t i = 0; i < count; ++i) destination[i] += source[i];
+  });
 }
 
 int c8r_total_bins(const c8r_accumulator* handle, size_t* coreas_bins, size_t* zhs_bins) {

@@ -1332,6 +1332,39 @@ __global__ void decode_kernel(const long long* __restrict__ fixed, double* __res
   }
 }
 
+// The output step on the device: CoREAS fields added as they are, ZHS
+// potentials differentiated into fields E_i = -(A_{i+1} - A_i) fs at the bin
+// midpoints (RadioProcess.inl:213-223; one sample fewer per observer), both
+// added into `out` (the observer add of CorsikaOutputSink.inl:255-278).
+// Values are the decoded traces: fixed x factor of the observer, or the FP64
+// traces.  `out` rows are [X | Y | Z] of total_bins - observers (ZHS) or
+// total_bins (CoREAS) values.
+__global__ void output_kernel(const long long* __restrict__ fixed, const double* __restrict__ floating,
+                              double* __restrict__ out, uint64_t total_bins,
+                              const ObserverCache* __restrict__ observers, const double* __restrict__ factors,
+                              uint32_t observer_count, int differentiate) {
+  uint32_t const o = blockIdx.y;
+  ObserverCache const& oc = observers[o];
+  double const f = fixed ? factors[o] : 1.;
+  uint64_t const bins = oc.bins;
+  uint64_t const samples = differentiate ? (bins > 0 ? bins - 1 : 0) : bins;
+  uint64_t const out_total = differentiate ? total_bins - observer_count : total_bins;
+  uint64_t const out_offset = differentiate ? oc.offset - o : oc.offset;
+  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < samples;
+       i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    for (int r = 0; r < 3; ++r) {
+      uint64_t const j = r * total_bins + oc.offset + i;
+      double const a = fixed ? static_cast<double>(fixed[j]) * f : floating[j];
+      double value = a;
+      if (differentiate) {
+        double const b = fixed ? static_cast<double>(fixed[j + 1]) * f : floating[j + 1];
+        value = -(b - a) * oc.sample_rate;
+      }
+      out[r * out_total + out_offset + i] += value;
+    }
+  }
+}
+
 template <bool kFixed, class Amp>
 cudaError_t direct_dispatch(EventPlan const& ev, uint64_t bound, bool coreas, bool zhs,
                             cudaStream_t stream) {
@@ -1445,6 +1478,19 @@ int windowed_ctas_per_sm(int window, int threads, bool fixed, Precision precisio
                                          : ctas_per_sm<true, float>(window, threads);
   return precision == Precision::kFP64 ? ctas_per_sm<false, double>(window, threads)
                                        : ctas_per_sm<false, float>(window, threads);
+}
+
+cudaError_t launch_output(const long long* fixed, const double* floating, double* out, uint64_t total_bins,
+                          const ObserverCache* observers, const double* factors, uint32_t observer_count,
+                          uint64_t max_bins, bool differentiate, cudaStream_t stream) {
+  if (observer_count == 0 || total_bins == 0) return cudaSuccess;
+  uint64_t bx = (max_bins + 255) / 256;
+  if (bx > 64) bx = 64;
+  if (bx == 0) bx = 1;
+  dim3 const grid(static_cast<unsigned>(bx), observer_count);
+  output_kernel<<<grid, 256, 0, stream>>>(fixed, floating, out, total_bins, observers, factors,
+                                          observer_count, differentiate ? 1 : 0);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_decode(const long long* fixed, double* out, uint64_t total_bins,

@@ -102,6 +102,12 @@ enum class TimeArithmetic : int { kDouble = 0, kDoubleFloat = 1, kFloat = 2 };
 cudaError_t launch_study(EventPlan const& event, uint64_t track_bound, bool coreas, bool zhs,
                          bool fixed, TimeArithmetic arithmetic, cudaStream_t stream);
 
+// Output step: decoded CoREAS fields, or ZHS fields -(A[i+1] - A[i]) fs,
+// added into `out` (fixed traces when `fixed` is non-null, else `floating`).
+cudaError_t launch_output(const long long* fixed, const double* floating, double* out, uint64_t total_bins,
+                          const ObserverCache* observers, const double* factors, uint32_t observer_count,
+                          uint64_t max_bins, bool differentiate, cudaStream_t stream);
+
 // Fixed-point decode on the device: out[r*bins + i] = in[r*bins + i] * factor(observer).
 cudaError_t launch_decode(const long long* fixed, double* out, uint64_t total_bins,
                           const uint64_t* observer_offsets, const double* factors,

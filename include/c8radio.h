@@ -318,6 +318,21 @@ int c8r_batch_autotune(c8r_batch* batch, c8r_accumulator* const* events, size_t 
                        int repetitions, c8r_tuning* best, double* best_ms);
 int c8r_batch_graph_captures(const c8r_batch* batch, unsigned long long* captures);
 
+/* ---- Output step on the device ----------------------------------------------
+ * RadioProcess.inl:213-223 and CorsikaOutputSink.inl:255-278: like c8r_download,
+ * but the decoded CoREAS fields (V/m, rows [X | Y | Z] of the CoREAS total bins)
+ * and the ZHS fields E_i = -(A_{i+1} - A_i) fs at the bin midpoints (V/m, one
+ * sample fewer per observer: rows of zhs total bins - zhs observers) are ADDED
+ * into caller-owned device buffers, so the waveforms of many showers sum on the
+ * device before one copy to the host.  Seals the accumulator as download does. */
+int c8r_download_fields_device(c8r_accumulator* handle, double* coreas_field_xyz, double* zhs_field_xyz,
+                               c8r_counters* counters);
+/* merge_fixed_accumulators (FixedAccumulatorMerge.inl:12-29), the core of
+ * CooperativeRadioMerge::commit (CooperativeRadioMerge.inl:180-202):
+ * destination += source for int64 fixed-point snapshots of one layout, every
+ * bin checked first; C8R_OVERFLOW_ERROR (nothing written) on overflow. */
+int c8r_merge_fixed(long long* destination, const long long* source, size_t count);
+
 /* ---- Track spool, version 1: completed host tracks on disk ----------------
  * corsika/kokkos/radio/RadioTrackSpoolFormat.hpp:24-29 and
  * RadioTrackSpool{Reader,Writer}.hpp: a 32-byte header ("C8_RADIO_TRACKS\0",

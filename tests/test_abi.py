@@ -104,3 +104,17 @@ def test_null_handles_are_rejected(pkg):
     assert lib.c8r_flush(None) == pkg.abi.C8R_INVALID_ARGUMENT
     assert lib.c8r_server_close(None, 1) == pkg.abi.C8R_INVALID_ARGUMENT
     assert b"null radio server" in lib.c8r_server_last_error(None)
+
+
+def test_fixed_snapshot_merge_is_checked_before_writing(pkg):
+    """merge_fixed_accumulators (FixedAccumulatorMerge.inl:21-28): an overflow in
+    any bin leaves the destination untouched."""
+    destination = np.array([1, 2 ** 62, -5, -(2 ** 62)], np.int64)
+    before = destination.copy()
+    with pytest.raises(pkg.OverflowErrorRadio):
+        pkg.merge_fixed(destination, np.array([2, 2 ** 62, 5, 0], np.int64))
+    assert np.array_equal(destination, before)
+    with pytest.raises(pkg.OverflowErrorRadio):
+        pkg.merge_fixed(destination, np.array([0, 0, 0, -(2 ** 62) - 1], np.int64))
+    pkg.merge_fixed(destination, np.array([2, 1, 5, -(2 ** 62)], np.int64))
+    assert destination.tolist() == [3, 2 ** 62 + 1, 0, -(2 ** 63)]
