@@ -356,6 +356,19 @@ class RadioAccumulator:
     def set_kernel_timing(self, enabled: bool) -> None:
         self._check(self._lib.c8r_set_kernel_timing(self._h, int(enabled)))
 
+    def accumulate_columns(self, columns: dict, count: int) -> None:
+        """accumulateLeptonTracks over device columns: a dict of device pointers
+        ('pid', 'weight', 'start_time_s', 'end_time_s', 'start_energy_gev', and
+        3-tuples 'start_position_m', 'end_position_m', 'start_direction',
+        'end_direction')."""
+        c = abi.TrackColumns()
+        for name in ("pid", "weight", "start_time_s", "end_time_s", "start_energy_gev"):
+            setattr(c, name, columns.get(name) or None)
+        for name in ("start_position_m", "end_position_m", "start_direction", "end_direction"):
+            values = columns.get(name) or (None, None, None)
+            setattr(c, name, (C.c_void_p * 3)(*values))
+        self._check(self._lib.c8r_accumulate_columns(self._h, C.byref(c), count))
+
     def download_fields_device(self, coreas_pointer: Optional[int], zhs_pointer: Optional[int]) -> dict:
         """Adds the decoded CoREAS fields (3 x coreas_bins doubles) and the ZHS
         fields -(A[i+1] - A[i]) fs (3 x (zhs_bins - zhs observers) doubles) into

@@ -221,6 +221,13 @@ TRACK_SEGMENT = np.dtype([
 assert TRACK_SEGMENT.itemsize == 144
 
 
+class TrackColumns(C.Structure):
+    _fields_ = [("pid", C.c_void_p), ("weight", C.c_void_p), ("start_time_s", C.c_void_p),
+                ("end_time_s", C.c_void_p), ("start_energy_gev", C.c_void_p),
+                ("start_position_m", C.c_void_p * 3), ("end_position_m", C.c_void_p * 3),
+                ("start_direction", C.c_void_p * 3), ("end_direction", C.c_void_p * 3)]
+
+
 class ServerOptions(C.Structure):
     _fields_ = [
         ("budget_bytes", C.c_uint64),
@@ -305,6 +312,7 @@ PROTOTYPES = {
     "c8r_server_fetch": (C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p,
                                    C.POINTER(Counters), C.POINTER(ServerEventInfo)]),
     "c8r_server_get_stats": (C.c_int, [C.c_void_p, C.POINTER(ServerStats)]),
+    "c8r_accumulate_columns": (C.c_int, [C.c_void_p, C.POINTER(TrackColumns), C.c_size_t]),
     "c8r_download_fields_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(Counters)]),
     "c8r_merge_fixed": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t]),
     "c8r_spool_writer_create": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),

@@ -373,6 +373,32 @@ class Accumulator {
     downloaded_ = false;
   }
 
+  // The same over a structure-of-arrays view of device steps, then projected.
+  void accumulate_columns(c8r_track_columns const& columns, std::size_t count) {
+    if (!enabled() || count == 0) return;
+    if (sealed_) throw std::logic_error("radio endpoint already committed; reset before new tracks");
+    bool ok = columns.pid && columns.weight && columns.start_time_s && columns.end_time_s;
+    for (int a = 0; a < 3; ++a) ok = ok && columns.start_position_m[a] && columns.end_position_m[a];
+    if (diagnostics_) {
+      ok = ok && columns.start_energy_gev;
+      for (int a = 0; a < 3; ++a) ok = ok && columns.start_direction[a] && columns.end_direction[a];
+    }
+    if (!ok) throw std::invalid_argument("null device radio track column");
+    if (staged_ > std::numeric_limits<std::size_t>::max() - count)
+      throw std::length_error("radio staged track count overflow");
+    ensure_capacity(staged_ + count);
+    if (staged_ == 0) check(cudaMemsetAsync(slot_.ptr, 0, sizeof(unsigned long long), stream_), "memset");
+    check(launch_ingest_columns(columns, count, tracks_.ptr, capacity_, slot_.ptr, counters_.ptr, diagnostics_,
+                                stream_),
+          "ingest launch");
+    staged_ += count;
+    ++stats_.track_precompute_batches;
+    stats_.track_precomputed_records += count;
+    stats_.maximum_track_batch = std::max<uint64_t>(stats_.maximum_track_batch, count);
+    downloaded_ = false;
+    project_staged(true);
+  }
+
   // Projects the staged tracks of this accumulator alone; consume drops them.
   void project_staged(bool consume) {
     if (!enabled() || staged_ == 0) return;
@@ -1265,6 +1291,14 @@ int c8r_download_fixed(c8r_accumulator* handle, long long* coreas_xyz, long long
   if (int s = with_handle(handle, nullptr, true)) return s;
   return guarded(&handle->error,
                  [&] { handle->impl->download_fixed(coreas_xyz, zhs_xyz, counters); });
+}
+
+int c8r_accumulate_columns(c8r_accumulator* handle, const c8r_track_columns* columns, size_t count) {
+  if (int s = with_handle(handle, nullptr, true)) return s;
+  return guarded(&handle->error, [&] {
+    if (!columns) throw std::invalid_argument("null radio track columns");
+    handle->impl->accumulate_columns(*columns, count);
+  });
 }
 
 int c8r_download_fields_device(c8r_accumulator* handle, double* coreas_field_xyz, double* zhs_field_xyz,

@@ -974,30 +974,55 @@ __device__ __forceinline__ int energy_bin(double kinetic) {
 }
 
 // ---------------------------------------------------------------- ingest
+// The fields radio reads from a track step, from 752-byte records or from
+// columns (one device array per field): the same arithmetic follows.
+struct RecordSource {
+  const c8r_lepton_transport_record* records;
+  __device__ int pid(uint64_t i) const { return records[i].start.pid; }
+  __device__ double weight(uint64_t i) const { return records[i].start.weight; }
+  __device__ double start_energy(uint64_t i) const { return records[i].start.energy_gev; }
+  __device__ double start_position(uint64_t i, int a) const { return records[i].start.position_m[a]; }
+  __device__ double end_position(uint64_t i, int a) const { return records[i].end.position_m[a]; }
+  __device__ double start_time(uint64_t i) const { return records[i].start.time_s; }
+  __device__ double end_time(uint64_t i) const { return records[i].end.time_s; }
+  __device__ double start_direction(uint64_t i, int a) const { return records[i].start.direction[a]; }
+  __device__ double end_direction(uint64_t i, int a) const { return records[i].end.direction[a]; }
+};
+
+struct ColumnSource {
+  c8r_track_columns columns;
+  __device__ int pid(uint64_t i) const { return columns.pid[i]; }
+  __device__ double weight(uint64_t i) const { return columns.weight[i]; }
+  __device__ double start_energy(uint64_t i) const { return columns.start_energy_gev[i]; }
+  __device__ double start_position(uint64_t i, int a) const { return columns.start_position_m[a][i]; }
+  __device__ double end_position(uint64_t i, int a) const { return columns.end_position_m[a][i]; }
+  __device__ double start_time(uint64_t i) const { return columns.start_time_s[i]; }
+  __device__ double end_time(uint64_t i) const { return columns.end_time_s[i]; }
+  __device__ double start_direction(uint64_t i, int a) const { return columns.start_direction[a][i]; }
+  __device__ double end_direction(uint64_t i, int a) const { return columns.end_direction[a][i]; }
+};
+
+template <class Source>
 __global__ void __launch_bounds__(256) ingest_kernel(
-    const c8r_lepton_transport_record* __restrict__ records, uint64_t count,
-    double* __restrict__ tracks, uint64_t stride, unsigned long long* slot,
-    DeviceCounters* counters, int diagnostics) {
+    const __grid_constant__ Source src, uint64_t count, double* __restrict__ tracks, uint64_t stride,
+    unsigned long long* slot, DeviceCounters* counters, int diagnostics) {
   uint64_t const i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   bool valid = false;
   Track t;
   double duration = 0.;
-  c8r_particle_state const* s = nullptr;
-  c8r_particle_state const* e = nullptr;
+  int pid = 0;
   if (i < count) {
-    s = &records[i].start;
-    e = &records[i].end;
-    int const pid = s->pid;
+    pid = src.pid(i);
     // make_radio_track_kinematics, RadioProjection.inl:145-168
     if (pid == 11 || pid == -11) {
-      t.sx = s->position_m[0];
-      t.sy = s->position_m[1];
-      t.sz = s->position_m[2];
-      t.ex = e->position_m[0];
-      t.ey = e->position_m[1];
-      t.ez = e->position_m[2];
-      t.ts = s->time_s;
-      t.te = e->time_s;
+      t.sx = src.start_position(i, 0);
+      t.sy = src.start_position(i, 1);
+      t.sz = src.start_position(i, 2);
+      t.ex = src.end_position(i, 0);
+      t.ey = src.end_position(i, 1);
+      t.ez = src.end_position(i, 2);
+      t.ts = src.start_time(i);
+      t.te = src.end_time(i);
       duration = t.te - t.ts;
       double const dx = t.ex - t.sx, dy = t.ey - t.sy, dz = t.ez - t.sz;
       t.length = sqrt(dx * dx + dy * dy + dz * dz);
@@ -1008,7 +1033,7 @@ __global__ void __launch_bounds__(256) ingest_kernel(
         t.bz = dz / denominator;
         t.beta_module = t.length / (kSpeedOfLight * duration);
         double const charge = pid == 11 ? -kElementaryCharge : kElementaryCharge;
-        t.constant = charge * kEmConstant * s->weight;
+        t.constant = charge * kEmConstant * src.weight(i);
         valid = true;
       }
     }
@@ -1039,8 +1064,8 @@ __global__ void __launch_bounds__(256) ingest_kernel(
   int ebin = -1;
   double ebin_value = 0.;
   if (valid) {
-    double const weight = s->weight;
-    double const kinetic = s->energy_gev - kElectronMassGeV;
+    double const weight = src.weight(i);
+    double const kinetic = src.start_energy(i) - kElectronMassGeV;
     if (isfinite(t.length) && t.length > 0. && isfinite(weight) && !(weight < 0.) &&
         isfinite(kinetic) && !(kinetic < 0.)) {
       double const weighted_length = weight * t.length;
@@ -1049,7 +1074,7 @@ __global__ void __launch_bounds__(256) ingest_kernel(
       wl = weighted_length;
       ewl = weighted_length * kinetic;
       maxlen = t.length;
-      if (s->pid == 11) {
+      if (pid == 11) {
         el = weighted_length;
         sl = -weighted_length;
       } else {
@@ -1061,8 +1086,8 @@ __global__ void __launch_bounds__(256) ingest_kernel(
       double direction_dot = 0.;
       double delta[3];
       for (int axis = 0; axis < 3; ++axis) {
-        double const pre = s->direction[axis];
-        double const post = e->direction[axis];
+        double const pre = src.start_direction(i, axis);
+        double const post = src.end_direction(i, axis);
         direction_dot += pre * post;
         delta[axis] = post - pre;
       }
@@ -1075,7 +1100,7 @@ __global__ void __launch_bounds__(256) ingest_kernel(
       bdef = weighted_length * (1. - t.beta_module);
       tres = weight * residual;
       maxchg = change;
-      double const charge_sign = s->pid == 11 ? -1. : 1.;
+      double const charge_sign = pid == 11 ? -1. : 1.;
       sdx = charge_sign * weight * delta[0];
       sdy = charge_sign * weight * delta[1];
       sdz = charge_sign * weight * delta[2];
@@ -1437,8 +1462,18 @@ cudaError_t launch_ingest(const c8r_lepton_transport_record* records, uint64_t c
                           DeviceCounters* counters, bool diagnostics, cudaStream_t stream) {
   if (count == 0) return cudaSuccess;
   uint64_t const blocks = (count + 255) / 256;
-  ingest_kernel<<<static_cast<unsigned>(blocks), 256, 0, stream>>>(records, count, tracks, stride,
-                                                                   slot, counters, diagnostics);
+  ingest_kernel<RecordSource><<<static_cast<unsigned>(blocks), 256, 0, stream>>>(
+      RecordSource{records}, count, tracks, stride, slot, counters, diagnostics);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ingest_columns(c8r_track_columns const& columns, uint64_t count, double* tracks,
+                                  uint64_t stride, unsigned long long* slot, DeviceCounters* counters,
+                                  bool diagnostics, cudaStream_t stream) {
+  if (count == 0) return cudaSuccess;
+  uint64_t const blocks = (count + 255) / 256;
+  ingest_kernel<ColumnSource><<<static_cast<unsigned>(blocks), 256, 0, stream>>>(
+      ColumnSource{columns}, count, tracks, stride, slot, counters, diagnostics);
   return cudaGetLastError();
 }
 

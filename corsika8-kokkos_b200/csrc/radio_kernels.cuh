@@ -9,6 +9,7 @@
 
 struct c8r_lepton_transport_record;
 struct c8r_counters;
+struct c8r_track_columns;
 
 namespace c8r {
 
@@ -80,6 +81,11 @@ enum class Precision : int { kFP64 = 0, kMixed = 1 };
 cudaError_t launch_ingest(const c8r_lepton_transport_record* records, uint64_t count,
                           double* tracks, uint64_t stride, unsigned long long* slot,
                           DeviceCounters* counters, bool diagnostics, cudaStream_t stream);
+
+// The same ingest from a structure-of-arrays view of the steps.
+cudaError_t launch_ingest_columns(c8r_track_columns const& columns, uint64_t count, double* tracks,
+                                  uint64_t stride, unsigned long long* slot, DeviceCounters* counters,
+                                  bool diagnostics, cudaStream_t stream);
 
 // Direct pair kernel: one thread per (track, observer) pair, global atomics.
 // The valid-track count is read on the device; `track_bound` (the record

@@ -318,6 +318,27 @@ int c8r_batch_autotune(c8r_batch* batch, c8r_accumulator* const* events, size_t 
                        int repetitions, c8r_tuning* best, double* best_ms);
 int c8r_batch_graph_captures(const c8r_batch* batch, unsigned long long* captures);
 
+/* ---- Producer-side input: track steps as columns ----------------------------
+ * No counterpart in the reference, which reads the 752-byte records
+ * (LeptonCascade.inl:81-83).  A producer that keeps its steps as a structure
+ * of arrays passes one device array per field radio reads, and skips writing
+ * and reading the records: the ingest reads about 100 bytes a track, in
+ * coalesced columns.  Same kinematics, bit for bit, as from records.  The
+ * direction and start-energy columns are read only with track_diagnostics. */
+typedef struct c8r_track_columns {
+  const int32_t* pid;               /* start state's PDG id (11, -11; others skipped) */
+  const double* weight;             /* start state's weight */
+  const double* start_time_s;
+  const double* end_time_s;
+  const double* start_energy_gev;   /* total energy (diagnostics) */
+  const double* start_position_m[3];
+  const double* end_position_m[3];
+  const double* start_direction[3]; /* diagnostics */
+  const double* end_direction[3];   /* diagnostics */
+} c8r_track_columns;
+/* accumulateLeptonTracks over columns: count steps, stream ordered. */
+int c8r_accumulate_columns(c8r_accumulator* handle, const c8r_track_columns* columns, size_t count);
+
 /* ---- Output step on the device ----------------------------------------------
  * RadioProcess.inl:213-223 and CorsikaOutputSink.inl:255-278: like c8r_download,
  * but the decoded CoREAS fields (V/m, rows [X | Y | Z] of the CoREAS total bins)
