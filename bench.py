@@ -648,7 +648,7 @@ def run_e2e(pkg, showers, wl, records, precision, kernel, stream, args, torch, b
             max_over_ranks, world):
     """reset + enqueueHostLeptonTracks(pinned host records) + download(pinned traces)."""
     config = showers.make_config(wl, precision=precision, kernel=kernel)
-    tuning = pkg.TuningParameters(batch_size=1 << 18)
+    tuning = pkg.TuningParameters(batch_size=1 << 20)
     acc = pkg.RadioAccumulator(config, tuning, stream=stream.cuda_stream)
     cudart = torch.cuda.cudart()
     registered = cudart.cudaHostRegister(records.ctypes.data, records.nbytes, 0) == 0
