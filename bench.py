@@ -67,6 +67,10 @@ def parse_args():
     p.add_argument("--serve-events", type=int, default=40)
     p.add_argument("--serve-rate", type=float, default=20.0, help="Poisson arrivals per second")
     p.add_argument("--serve-budget-gb", type=float, default=120.0)
+    p.add_argument("--serve-round-pairs", type=int, default=0,
+                   help="server round size in track-observer pairs (0: the server's default)")
+    p.add_argument("--serve-chunk", type=int, default=0,
+                   help="server tracks per work item (0: the server's default)")
     p.add_argument("--library-segments", type=int, default=500_000,
                    help="segments of each of the 15 replayed library showers")
     p.add_argument("--batched", action="store_true",
@@ -380,7 +384,8 @@ def run_serving(pkg, showers, torch, args, local: int) -> dict:
     configs = [showers.make_config(showers.event_workload(spec)[0], precision=1, kernel=2)
                for spec in specs]
     torch.cuda.synchronize()
-    server = pkg.RadioServer(budget_bytes=int(args.serve_budget_gb * 1e9))
+    server = pkg.RadioServer(budget_bytes=int(args.serve_budget_gb * 1e9), round_pairs=args.serve_round_pairs,
+                             chunk_tracks=args.serve_chunk)
 
     def feed(event, spec, count, stream):
         base = dev[showers.library_key(spec)].data_ptr()

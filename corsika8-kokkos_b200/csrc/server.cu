@@ -188,8 +188,8 @@ class Server {
  public:
   explicit Server(c8r_server_options const& options) {
     block_tracks_ = options.block_tracks ? options.block_tracks : (1u << 20);
-    chunk_tracks_ = options.chunk_tracks ? options.chunk_tracks : 65536;
-    round_pairs_ = options.round_pairs ? options.round_pairs : 400000000ull;
+    chunk_tracks_ = options.chunk_tracks ? options.chunk_tracks : 131072;
+    round_pairs_ = options.round_pairs ? options.round_pairs : 1000000000ull;
     threads_ = options.team_size ? static_cast<int>(options.team_size) : kWindowThreads;
     if (chunk_tracks_ == 0 || chunk_tracks_ > 0x7fffffffu || block_tracks_ % chunk_tracks_ != 0 ||
         block_tracks_ / chunk_tracks_ > 0xffffffffu)
