@@ -93,10 +93,6 @@ __device__ __forceinline__ bool no_overflow3(unsigned long long px, long long x,
 struct GlobalSink {
   unsigned long long* row[3];
   double* frow[3];
-  __device__ __forceinline__ bool add(int c, uint64_t bin, long long v) {
-    return checked(atomicAdd(row[c] + bin, static_cast<unsigned long long>(v)), v);
-  }
-  __device__ __forceinline__ void addf(int c, uint64_t bin, double v) { atomicAdd(frow[c] + bin, v); }
   // All three components at one bin; false if a conversion failed or an add overflowed.
   __device__ __forceinline__ bool add3(uint64_t bin, long long x, long long y, long long z,
                                        bool ox, bool oy, bool oz, float mag, float& bound) {
@@ -140,18 +136,6 @@ struct WindowSink {
   bool unchecked;
   unsigned long long* row[3];
   double* frow[3];
-  __device__ __forceinline__ bool add(int c, uint64_t bin, long long v) {
-    unsigned long long const u = static_cast<unsigned long long>(v);
-    unsigned long long const previous =
-        bin < width ? atomicAdd(win + c * width + bin, u) : atomicAdd(row[c] + bin, u);
-    return checked(previous, v);
-  }
-  __device__ __forceinline__ void addf(int c, uint64_t bin, double v) {
-    if (bin < width)
-      atomicAdd(fwin + c * width + bin, v);
-    else
-      atomicAdd(frow[c] + bin, v);
-  }
   // unchecked: window adds whose results are not read; `bound` then gains
   // |x| + |y| + |z| (as `mag`), and the kernel checks afterwards that no
   // partial sum of the window can have left the int64 range.
