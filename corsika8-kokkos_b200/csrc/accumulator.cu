@@ -943,7 +943,7 @@ class Accumulator {
 };
 
 
-// Batched projection: the staged tracks of many
+// Batched projection (many showers per launch): the staged tracks of many
 // accumulators projected by one persistent launch per algorithm (up to
 // kMaxEventsPerLaunch events a launch), optionally replayed from a CUDA graph
 // captured per distinct launch plan.
