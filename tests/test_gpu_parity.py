@@ -285,6 +285,29 @@ def test_window_rerun_near_the_fixed_point_limit(pkg, oracle, showers, torch_cud
         assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_traces_longer_than_the_window(pkg, oracle, showers, torch_cuda, precision):
+    """20000-bin traces exceed the largest shared-memory window: the bins past
+    it go to checked global atomics, and such items never take unchecked window
+    adds.  FP64 traces equal the oracle's; mixed-precision bins equal FP64's."""
+    wl, records = _workload_records(showers, "plain_c0", 30_000, seed=14)
+    # the pulse arrives about 800 ns (bin ~8000) after each trace starts: it straddles the window edge
+    wl["observers"] = showers.star_antennas(4, [40.0, 120.0], 1400.0, 20000, 1e10, pre_trigger_s=800e-9)
+    count_cfg = showers.make_config(wl, precision=precision, kernel=2, count_samples=True)
+    got = gpu_project(pkg, torch_cuda, count_cfg, records)
+    want = oracle.restatement().project(showers.make_config(wl, count_samples=True), records, threads=8)
+    assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
+    # the window holds about 8400 bins on a B200 (227 KB of shared memory a block)
+    tail = got[0][0].reshape(8, 20000)[:, 8420:].sum() + got[1][0].reshape(8, 20000)[:, 8420:].sum()
+    head = got[0][0].reshape(8, 20000)[:, :8400].sum() + got[1][0].reshape(8, 20000)[:, :8400].sum()
+    assert tail > 0 and head > 0  # samples on both sides of the window edge
+    if precision == 0:
+        config = showers.make_config(wl, precision=0, kernel=2)
+        got = gpu_project(pkg, torch_cuda, config, records)
+        want = oracle.restatement().project(config, records, threads=8)
+        assert_same(got, want, True)
+
+
 def test_empty_and_repeated_batches(pkg, oracle, showers, torch_cuda):
     wl, records = _workload_records(showers, "plain_c0", 40_000, seed=4)
     config = showers.make_config(wl, kernel=2)
