@@ -14,6 +14,7 @@ package without the built library raises.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from dataclasses import dataclass, field
 from pathlib import Path
 from typing import Optional
@@ -24,7 +25,8 @@ from . import abi
 from .abi import LEPTON_RECORD, OBSERVER, PARTICLE_STATE  # noqa: F401
 
 HERE = Path(__file__).resolve().parent
-LIBRARY_PATH = HERE / "libc8radio.so"
+# C8R_LIBRARY selects another build of the library (A/B comparisons).
+LIBRARY_PATH = Path(os.environ["C8R_LIBRARY"]).resolve() if os.environ.get("C8R_LIBRARY") else HERE / "libc8radio.so"
 
 # ------------------------------------------------------------------ errors
 class RadioError(RuntimeError):
