@@ -179,7 +179,7 @@ std::size_t projected_device_bytes(c8r_config const& config) {
     total = checked_add(total, checked_mul(values, sizeof(long long)));
     total = checked_add(total, checked_mul(values, sizeof(double)));  // decode buffer
   }
-  total = checked_add(total, sizeof(DeviceCounters) + sizeof(unsigned long long) + sizeof(unsigned));
+  total = checked_add(total, sizeof(DeviceCounters) + sizeof(unsigned long long) + 2 * sizeof(unsigned));
   total = checked_add(total, checked_mul(kDefaultHostBatch, sizeof(c8r_lepton_transport_record)));
   return total;
 }
@@ -210,7 +210,7 @@ class Accumulator {
     allocate_traces();
     counters_.allocate(1);
     slot_.allocate(1);
-    next_item_.allocate(1);
+    next_item_.allocate(2);  // one work counter per algorithm
     staging_.allocate(host_batch_);
     for (auto& h : host_) h.allocate(host_batch_);
     for (auto& e : host_ready_) check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
@@ -225,6 +225,12 @@ class Accumulator {
       cudaStreamSynchronize(copy_stream_);
       cudaStreamDestroy(copy_stream_);
     }
+    if (side_stream_) {
+      cudaStreamSynchronize(side_stream_);
+      cudaStreamDestroy(side_stream_);
+    }
+    for (auto& e : side_events_)
+      if (e) cudaEventDestroy(e);
     for (auto& e : copy_done_)
       if (e) cudaEventDestroy(e);
     for (auto& e : consumed_)
@@ -264,12 +270,11 @@ class Accumulator {
     if (downloaded_ || sealed_) throw std::logic_error("radio already downloaded; reset before host tracks");
     if (count != 0 && records == nullptr) throw std::invalid_argument("null host radio track input");
     if (count >= host_batch_ && host_count_ == 0 && is_pinned(records)) {
-      // Page-locked caller memory: DMA whole batches straight from it, then
-      // wait for the copies before returning (the caller may reuse it).
-      std::size_t const whole = count - count % host_batch_;
-      enqueue_pinned(records, whole);
-      records += whole;
-      count -= whole;
+      // Page-locked caller memory: DMA every batch, the last partial one
+      // included, straight from it, then wait for the copies before
+      // returning (the caller may reuse it).
+      enqueue_pinned(records, count);
+      return;
     }
     while (count != 0) {
       if (host_count_ == 0) check(cudaEventSynchronize(host_ready_[host_index_]), "staging wait");
@@ -292,9 +297,13 @@ class Accumulator {
     return attributes.type == cudaMemoryTypeHost;
   }
 
-  // Batches of host_batch_ records copied from pinned caller memory into a
-  // pair of device staging buffers (copy of batch k+1 overlaps projection of
-  // batch k on the copy stream); returns after the last copy completed.
+  // Batches of host_batch_ records (the last one partial) copied from pinned
+  // caller memory into a pair of device staging buffers (copy of batch k+1
+  // overlaps projection of batch k on the copy stream); returns after the
+  // last copy completed.  The first four batches are 1/8, 1/8, 1/4 and 1/2 of
+  // host_batch_ (together one batch), so the projection starts after a short
+  // copy and each later copy still runs behind the projection of the batch
+  // before it.
   void enqueue_pinned(c8r_lepton_transport_record const* records, std::size_t count) {
     if (!copy_stream_) {
       check(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking), "copy stream");
@@ -304,23 +313,27 @@ class Accumulator {
     }
     // earlier work on the accumulator stream may still read staging_
     for (auto& e : consumed_) check(cudaEventRecord(e, stream_), "event");
-    std::size_t const batches = count / host_batch_;
-    for (std::size_t b = 0; b < batches; ++b) {
+    bool const ramp = host_batch_ % 8 == 0 && host_batch_ / 8 >= 8192;
+    std::size_t offset = 0;
+    for (std::size_t b = 0; offset < count; ++b) {
+      static constexpr int kRampShift[4] = {3, 3, 2, 1};
+      std::size_t const n =
+          std::min(count - offset, ramp && b < 4 ? host_batch_ >> kRampShift[b] : host_batch_);
       int const k = static_cast<int>(b & 1);
       c8r_lepton_transport_record* dst = k ? staging2_.ptr : staging_.ptr;
       // the staging buffer is free once the ingest that read it has run
       check(cudaStreamWaitEvent(copy_stream_, consumed_[k], 0), "wait");
-      check(cudaMemcpyAsync(dst, records + b * host_batch_,
-                            host_batch_ * sizeof(c8r_lepton_transport_record),
+      check(cudaMemcpyAsync(dst, records + offset, n * sizeof(c8r_lepton_transport_record),
                             cudaMemcpyHostToDevice, copy_stream_),
             "host track upload");
       check(cudaEventRecord(copy_done_[k], copy_stream_), "event");
       check(cudaStreamWaitEvent(stream_, copy_done_[k], 0), "wait");
-      accumulate_device(dst, host_batch_, host_batch_);
+      accumulate_device(dst, n, host_batch_);
       check(cudaEventRecord(consumed_[k], stream_), "event");
-      stats_.host_to_device_bytes += host_batch_ * sizeof(c8r_lepton_transport_record);
+      offset += n;
+      stats_.host_to_device_bytes += n * sizeof(c8r_lepton_transport_record);
       ++stats_.host_track_batches;
-      stats_.host_tracks_enqueued += host_batch_;
+      stats_.host_tracks_enqueued += n;
     }
     check(cudaStreamSynchronize(copy_stream_), "host track upload");
   }
@@ -810,6 +823,8 @@ class Accumulator {
     chunk = std::min<std::size_t>(chunk, 0x7fffffffu);
     ev.chunk_size = static_cast<uint32_t>(chunk);
     ev.chunks = static_cast<uint32_t>((count + chunk - 1) / chunk);
+    ev.first_track = 0;
+    ev.last_track = ~0ull;
     return ev;
   }
 
@@ -839,38 +854,54 @@ class Accumulator {
     stats_.direct_projection_records += count;
   }
 
-  // One persistent launch per algorithm (CoREAS items, then ZHS items): each
-  // kernel instance carries one algorithm's code only.
+  // One persistent launch per algorithm: each kernel instance carries one
+  // algorithm's code only.  CoREAS items run on stream_ and, when both
+  // algorithms are on, ZHS items on a second stream: both kernels hold one CTA
+  // per SM, so ZHS CTAs start on the SMs that the CoREAS launch's last items
+  // leave idle instead of after its slowest CTA.  stream_ then waits for both.
+  // With kernel timing on, both run on stream_, so that each launch's events
+  // bracket that launch alone.
   void project_windowed(std::size_t count) {
     EventPlan const ev = make_event(count);
     int per_sm = windowed_ctas_per_sm(static_cast<int>(ev.window), threads_, fixed_, precision_);
     if (per_sm <= 0) throw cuda_error("windowed radio kernel does not fit on this device");
+    bool const both = !timing_ && ev.observer_count[0] != 0 && ev.observer_count[1] != 0;
+    if (both) {
+      if (!side_stream_) {
+        check(cudaStreamCreateWithFlags(&side_stream_, cudaStreamNonBlocking), "side stream");
+        for (auto& e : side_events_) check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+      }
+      check(cudaEventRecord(side_events_[0], stream_), "event");
+      check(cudaStreamWaitEvent(side_stream_, side_events_[0], 0), "wait");
+    }
     for (int algorithm = 0; algorithm < 2; ++algorithm) {
       if (ev.observer_count[algorithm] == 0) continue;
+      cudaStream_t const s = both && algorithm == 1 ? side_stream_ : stream_;
       WorkPlan plan{};
-      plan.events[0] = ev;
-      plan.events[0].first_item = 0;
       plan.algorithm = algorithm;
-      plan.event_count = 1;
       plan.window = ev.window;
-      plan.total_items = static_cast<uint64_t>(ev.chunks) * ev.observer_count[algorithm];
-      plan.next_item = next_item_.ptr;
+      plan.next_item = next_item_.ptr + algorithm;
       uint64_t ctas = static_cast<uint64_t>(per_sm) * sms_;
+      append_work(plan, ev, ctas, true);
       if (ctas > plan.total_items) ctas = plan.total_items;
-      check(cudaMemsetAsync(next_item_.ptr, 0, sizeof(unsigned), stream_), "memset");
+      check(cudaMemsetAsync(plan.next_item, 0, sizeof(unsigned), s), "memset");
       cudaEvent_t b = nullptr, e = nullptr;
       if (timing_) {
         b = timing_event();
-        check(cudaEventRecord(b, stream_), "event");
+        check(cudaEventRecord(b, s), "event");
       }
-      check(launch_windowed(plan, fixed_, precision_, static_cast<int>(ctas), threads_, stream_),
+      check(launch_windowed(plan, fixed_, precision_, static_cast<int>(ctas), threads_, s),
             "windowed launch");
       if (timing_) {
         e = timing_event();
-        check(cudaEventRecord(e, stream_), "event");
+        check(cudaEventRecord(e, s), "event");
         pending_.push_back({{b, e}, algorithm});
       }
       stats_.projection_tiles += plan.total_items;
+    }
+    if (both) {
+      check(cudaEventRecord(side_events_[1], side_stream_), "event");
+      check(cudaStreamWaitEvent(stream_, side_events_[1], 0), "wait");
     }
     uint64_t const pairs_c = count * ev.observer_count[0];
     uint64_t const pairs_z = count * ev.observer_count[1];
@@ -930,6 +961,8 @@ class Accumulator {
   cudaStream_t copy_stream_ = nullptr;
   cudaEvent_t copy_done_[2] = {nullptr, nullptr};
   cudaEvent_t consumed_[2] = {nullptr, nullptr};
+  cudaStream_t side_stream_ = nullptr;               // ZHS launches beside CoREAS
+  cudaEvent_t side_events_[2] = {nullptr, nullptr};  // tracks ingested, ZHS done
   PinnedBuffer<c8r_lepton_transport_record> host_[2];
   cudaEvent_t host_ready_[2] = {nullptr, nullptr};
   // (begin, end) event pairs; tag -1 = a whole accumulate's projection,
@@ -1097,21 +1130,18 @@ class Batch {
         l.plan.window = window;
         l.plan.next_item = next_item_.ptr;
         l.threads = threads;
-        uint64_t items = 0;
-        std::size_t j = first;
-        for (; j < active.size() && l.plan.event_count < static_cast<uint32_t>(kMaxEventsPerLaunch); ++j) {
-          EventPlan ev = active[j].second;
-          if (ev.observer_count[algorithm] == 0) continue;
-          ev.first_item = items;
-          uint64_t const event_items = static_cast<uint64_t>(ev.chunks) * ev.observer_count[algorithm];
-          items += event_items;
-          out.items[active[j].first] += event_items;
-          l.plan.events[l.plan.event_count++] = ev;
-        }
-        first = j;
-        if (l.plan.event_count == 0) continue;
-        l.plan.total_items = items;
         uint64_t ctas = static_cast<uint64_t>(per_sm) * sms;
+        // the events of this launch; the last one ends the work list on short items
+        std::vector<std::size_t> members;
+        std::size_t j = first;
+        for (; j < active.size() && members.size() < static_cast<std::size_t>(kMaxEventsPerLaunch); ++j)
+          if (active[j].second.observer_count[algorithm] != 0) members.push_back(j);
+        first = j;
+        if (members.empty()) continue;
+        for (std::size_t m = 0; m < members.size(); ++m)
+          out.items[active[members[m]].first] +=
+              append_work(l.plan, active[members[m]].second, ctas, m + 1 == members.size());
+        uint64_t const items = l.plan.total_items;
         if (ctas > items) ctas = items;
         l.ctas = static_cast<int>(ctas);
         out.launches.push_back(l);

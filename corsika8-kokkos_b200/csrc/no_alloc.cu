@@ -230,6 +230,8 @@ void accumulate_no_alloc(c8r_config const& config, c8r_lepton_transport_record c
   ev.propagation = prop;
   ev.counters = event_counters;
   ev.window = window;
+  ev.first_track = 0;
+  ev.last_track = ~0ull;
 
   // records in chunks of at most kTrackCapacity: ingest into the scratch
   // kinematics, then one persistent launch per algorithm over the chunk

@@ -1204,9 +1204,9 @@ __global__ void __launch_bounds__(kAlgorithm == 1 ? kZhsThreadsMax : kWindowThre
     uint32_t const per_chunk = ev.observer_count[algorithm];
     uint64_t const slice_chunk = local / per_chunk;
     uint32_t const oi = static_cast<uint32_t>(local - slice_chunk * per_chunk);
-    uint64_t const chunk = ev.chunk_begin + slice_chunk;
-    uint64_t const track_count = *ev.valid_tracks;
-    uint64_t const begin = chunk * ev.chunk_size;
+    uint64_t const valid = *ev.valid_tracks;
+    uint64_t const track_count = valid < ev.last_track ? valid : ev.last_track;
+    uint64_t const begin = ev.first_track + slice_chunk * ev.chunk_size;
     if (begin >= track_count) continue;
     uint64_t const end = begin + ev.chunk_size < track_count ? begin + ev.chunk_size : track_count;
     if (threadIdx.x == 0) observer = ev.observers[algorithm][oi];

@@ -56,22 +56,66 @@ struct EventPlan {
   uint32_t chunk_size;           // tracks per work item
   uint32_t chunks;
   uint32_t window;               // shared-memory bins per item (<= kernel window)
-  uint32_t chunk_begin;          // first chunk of this plan (a slice of the tracks)
+  uint64_t first_track;          // chunk c covers first_track + c * chunk_size onwards,
+  uint64_t last_track;           // clipped to [.., last_track) and the valid tracks
 };
 
 // Persistent windowed launch over a work list of (event, chunk, algorithm,
 // observer) items drawn from an atomic counter.  Passed as a __grid_constant__
 // kernel parameter (no host-to-device copy; graph-capturable).
 constexpr int kMaxEventsPerLaunch = 64;
+constexpr int kPlanEntries = kMaxEventsPerLaunch + 1;  // + the short-chunk tail of the last event
 constexpr int kWindowThreads = 640;  // upper bound (and default) of the windowed block size
 struct WorkPlan {
-  EventPlan events[kMaxEventsPerLaunch];
+  EventPlan events[kPlanEntries];
   int32_t algorithm;        // 0: CoREAS items, 1: ZHS items
   uint32_t event_count;
   uint32_t window;          // shared-memory bins per CTA (max over events)
   uint64_t total_items;
   unsigned int* next_item;  // zeroed before each launch
 };
+
+// Appends the (chunk, observer) work items of `ev` for plan.algorithm to
+// `plan` (first_item, event_count and total_items follow).  With `fine_tail`
+// and a free event slot, the last chunks go in as a second entry of chunks a
+// quarter as long (at least 8192 tracks), about two items for each of the
+// `ctas` persistent CTAs: the launch then ends on short items instead of one
+// CTA finishing a long item while the others wait.  Every track stays in
+// exactly one item.  Returns the number of items appended.
+inline uint64_t append_work(WorkPlan& plan, EventPlan ev, uint64_t ctas, bool fine_tail) {
+  constexpr uint64_t kSplit = 4, kMinTailChunk = 8192;
+  uint64_t const per = ev.observer_count[plan.algorithm];
+  if (per == 0 || ev.chunks == 0 || plan.event_count >= kPlanEntries) return 0;
+  uint64_t const big = ev.chunk_size;
+  uint64_t const small = (big + kSplit - 1) / kSplit > kMinTailChunk ? (big + kSplit - 1) / kSplit
+                                                                     : kMinTailChunk;
+  uint64_t head = ev.chunks;
+  if (fine_tail && plan.event_count + 2 <= kPlanEntries && small < big) {
+    uint64_t const short_items = (2 * ctas + per - 1) / per;
+    uint64_t const replaced = (short_items * small + big - 1) / big;  // long chunks they cover
+    head = replaced >= ev.chunks ? 0 : ev.chunks - replaced;
+  }
+  uint64_t const before = plan.total_items;
+  if (head > 0) {
+    EventPlan e = ev;
+    e.chunks = static_cast<uint32_t>(head);
+    e.first_item = plan.total_items;
+    plan.events[plan.event_count++] = e;
+    plan.total_items += head * per;
+  }
+  if (head < ev.chunks) {
+    uint64_t const stop = ev.first_track + ev.chunks * big;
+    EventPlan e = ev;
+    e.first_track = ev.first_track + head * big;
+    e.last_track = stop < ev.last_track ? stop : ev.last_track;
+    e.chunk_size = static_cast<uint32_t>(small);
+    e.chunks = static_cast<uint32_t>(((ev.chunks - head) * big + small - 1) / small);
+    e.first_item = plan.total_items;
+    plan.events[plan.event_count++] = e;
+    plan.total_items += static_cast<uint64_t>(e.chunks) * per;
+  }
+  return plan.total_items - before;
+}
 
 enum class Precision : int { kFP64 = 0, kMixed = 1 };
 

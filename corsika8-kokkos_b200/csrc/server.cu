@@ -705,11 +705,12 @@ class Server {
         std::memset(&plan, 0, sizeof plan);
         plan.algorithm = a;
         uint32_t window = 1;
-        uint64_t items = 0;
+        std::vector<EventPlan> members;
         for (Slice const& s : slices) {
           ServedEvent const& ev = *s.event;
           if (ev.fixed != fixed || ev.precision != precision || ev.observers[a] == 0) continue;
-          EventPlan& e = plan.events[plan.event_count++];
+          EventPlan e;
+          std::memset(&e, 0, sizeof e);
           e.tracks = s.block->tracks;
           e.stride = block_tracks_;
           e.valid_tracks = s.block->slot;
@@ -722,20 +723,23 @@ class Server {
           }
           e.propagation = ev.propagation;
           e.counters = ev.counters;
-          e.first_item = items;
           e.chunk_size = static_cast<uint32_t>(chunk_tracks_);
           e.chunks = s.chunks;
-          e.chunk_begin = s.chunk_begin;
+          e.first_track = static_cast<uint64_t>(s.chunk_begin) * chunk_tracks_;
+          e.last_track = e.first_track + static_cast<uint64_t>(s.chunks) * chunk_tracks_;
           e.window = ev.window;
           window = std::max(window, ev.window);
-          items += static_cast<uint64_t>(s.chunks) * ev.observers[a];
+          members.push_back(e);
         }
-        if (plan.event_count == 0) continue;
+        if (members.empty()) continue;
         unsigned* const counter = next_item_ + (stats_.launches % 64);
         plan.window = window;
-        plan.total_items = items;
         plan.next_item = counter;
         uint64_t ctas = static_cast<uint64_t>(ctas_per_sm(window, fixed, precision)) * sms_;
+        // the last slice ends the round's work list on short items
+        for (std::size_t m = 0; m < members.size(); ++m)
+          append_work(plan, members[m], ctas, m + 1 == members.size());
+        uint64_t const items = plan.total_items;
         if (ctas > items) ctas = items;
         check(cudaMemsetAsync(counter, 0, sizeof(unsigned), compute_), "server work counter");
         check(launch_windowed(plan, fixed, precision, static_cast<int>(ctas), threads_, compute_),

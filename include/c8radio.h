@@ -275,7 +275,9 @@ int c8r_projected_track_capacity(const c8r_accumulator* handle, size_t count,
                                  size_t* retained_bytes, size_t* transient_peak_bytes);
 /* B200 extension: when enabled, each accumulate records CUDA events around
  * its projection kernels (no host synchronisation); c8r_get_statistics sums
- * the elapsed times of completed launches into kernel_time_ms. */
+ * the elapsed times of completed launches into kernel_time_ms.  The CoREAS
+ * and ZHS launches then run one after the other on the accumulator's stream
+ * (otherwise the ZHS launch runs beside the CoREAS one on a second stream). */
 int c8r_set_kernel_timing(c8r_accumulator* handle, int enabled);
 /* B200 extension, no reference counterpart: measures the rates of c8r_peaks
  * on the current device (a few milliseconds of probe kernels). */

@@ -187,6 +187,36 @@ def test_host_enqueue_batches_match_device_path(pkg, oracle, showers, torch_cuda
         assert stats.host_tracks_enqueued == sum(p.size for p in pieces)
 
 
+def test_short_tail_items_and_ramped_pinned_batches(pkg, oracle, showers, torch_cuda):
+    """Work lists that end on quarter-size chunks (the last large chunk split in
+    four) and pinned host input copied straight from the caller's memory in
+    batches of 1/8, 1/8, 1/4, 1/2 and then whole host batches (the last one
+    partial) give the traces of one plain device launch."""
+    wl, records = _workload_records(showers, "tiled_c1", 100_000, seed=41)
+    want = oracle.restatement().project(showers.make_config(wl), records, threads=16)
+    pinned = torch_cuda.empty(records.nbytes, dtype=torch_cuda.uint8, pin_memory=True).numpy()
+    pinned[:] = records.view(np.uint8)
+    host = pinned.view(pkg.LEPTON_RECORD)
+    for precision in (0, 1):
+        config = showers.make_config(wl, precision=precision, kernel=KERNELS["windowed"])
+        plain = gpu_project(pkg, torch_cuda, config, records)
+        if precision == 0:
+            assert_same(plain, want, True)
+        # 32768-track items: three long chunks, then four of 8192 tracks
+        tiled = gpu_project(pkg, torch_cuda, config, records,
+                            tuning=pkg.TuningParameters(track_tile_size=32768))
+        assert_same(tiled, plain, True)
+        acc = pkg.RadioAccumulator(config, pkg.TuningParameters(batch_size=65536,
+                                                                track_tile_size=32768))
+        acc.enqueue_host_lepton_tracks(host)
+        got = acc.download_fixed()
+        stats = acc.statistics()
+        acc.close()
+        assert_same(got, plain, True)
+        # 8192 + 8192 + 16384 + 32768, then a last partial batch of 34464
+        assert stats.host_track_batches == 5 and stats.host_tracks_enqueued == records.size
+
+
 def test_lifecycle_contracts(pkg, showers, torch_cuda):
     """Rejection contracts of testRadioAccumulator.cpp:216-302."""
     wl, records = _workload_records(showers, "plain_c0", 100, seed=1)
