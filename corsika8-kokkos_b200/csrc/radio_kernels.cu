@@ -1168,7 +1168,6 @@ constexpr int kWindowThreadsMax = kWindowThreads;
 // 384-thread CTAs (up to 168 registers, no spills).
 constexpr int kZhsThreadsMax = 384;
 constexpr unsigned kWarpQueue = 64;  // entries per warp: < 32 kept + 32 pushed per round
-constexpr int kFlushDepth = 8;       // window flush: global adds in flight per thread
 constexpr size_t kQueueBytes = (kWindowThreadsMax / 32) * kWarpQueue * sizeof(unsigned);
 // staging slots of the ZHS kernel: 32 per warp, sized for the FP64 amplitudes
 constexpr size_t kStagingBytes = (kZhsThreadsMax / 32) * 32 * sizeof(StagedSegment<double>);
@@ -1310,32 +1309,17 @@ __global__ void __launch_bounds__(kAlgorithm == 1 ? kZhsThreadsMax : kWindowThre
       c = saved;
     }
 
-    // flush: non-zero bins, checked global adds, kFlushDepth of them in
-    // flight per thread before their previous values are tested
-    for (int row = 0; row < 3; ++row) {
-      unsigned long long const* const src = window + static_cast<size_t>(row) * width;
-      for (uint32_t b0 = threadIdx.x; b0 < width; b0 += kFlushDepth * blockDim.x) {
-        unsigned long long v[kFlushDepth], previous[kFlushDepth];
-#pragma unroll
-        for (int u = 0; u < kFlushDepth; ++u) {
-          uint32_t const bin = b0 + u * blockDim.x;
-          v[u] = bin < width ? src[bin] : 0ull;
-        }
-#pragma unroll
-        for (int u = 0; u < kFlushDepth; ++u) {
-          uint32_t const bin = b0 + u * blockDim.x;
-          previous[u] = 0ull;
-          if (v[u] == 0ull) continue;
-          if (kFixed)
-            previous[u] = atomicAdd(sink.row[row] + bin, v[u]);
-          else
-            atomicAdd(sink.frow[row] + bin, __longlong_as_double(static_cast<long long>(v[u])));
-        }
-        if (kFixed) {
-#pragma unroll
-          for (int u = 0; u < kFlushDepth; ++u)
-            if (v[u] != 0ull && !checked(previous[u], static_cast<long long>(v[u]))) ++c.overflows;
-        }
+    // flush: non-zero bins, checked global adds
+    for (uint32_t j = threadIdx.x; j < 3 * width; j += blockDim.x) {
+      unsigned long long const v = window[j];
+      if (v == 0ull) continue;
+      uint32_t const row = j / width;
+      uint32_t const bin = j - row * width;
+      if (kFixed) {
+        long long const inc = static_cast<long long>(v);
+        if (!checked(atomicAdd(sink.row[row] + bin, v), inc)) ++c.overflows;
+      } else {
+        atomicAdd(sink.frow[row] + bin, __longlong_as_double(static_cast<long long>(v)));
       }
     }
     flush_counts(c, ev.counters);
