@@ -184,6 +184,87 @@ __device__ __forceinline__ Path propagate(Propagation const& p, ObserverCache co
   return r;
 }
 
+// propagate (RadioProjection.inl:170-238) for the filtered decisions of the
+// mixed-precision path.  The refractive indices and the integral ratio
+// (i_src - i_dst) / height are the reference's (same table reads, same IEEE
+// division); 1/|d| is an FP32 reciprocal square root refined by two Newton
+// steps in FP64, |d| = RN(|d|^2 (1/|d|)), k = d (1/|d|), and the travel time
+// multiplies by RN(1/c) instead of dividing by c.  With the final Newton
+// residual r = 1 - |d|^2 y^2, y lies within |r|/2 + u of 1/|d| (u = 2^-53);
+// `ok` requires |r| <= 2^-50, so y is within 5u, each direction component
+// within 8u |k| of the reference's, and the time within 12u |time|
+// (|d| within 7u, two products and RN(1/c) against one division):
+// `time_err` = 2^-48 |time| (32u).  `ok` is false (the caller evaluates
+// exactly) when |d|^2 lies outside [2^-100, 2^100], the residual is larger or
+// the time is not finite.
+struct FastPath {
+  double time, n_src, n_dst, dist, kx, ky, kz, time_err;
+  bool ok;
+};
+
+__device__ __forceinline__ FastPath propagate_fast(Propagation const& p, ObserverCache const& o,
+                                                   double sx, double sy, double sz) {
+  FastPath r;
+  double const dx = o.px - sx, dy = o.py - sy, dz = o.pz - sz;
+  double const s2 = dx * dx + dy * dy + dz * dz;
+  r.ok = s2 >= 0x1p-100 && s2 <= 0x1p100;
+  double y = static_cast<double>(rsqrtf(static_cast<float>(r.ok ? s2 : 1.)));
+#pragma unroll
+  for (int step = 0; step < 2; ++step) {
+    double const h = s2 * y;
+    y = fma(0.5 * y, fma(-h, y, 1.), y);
+  }
+  double const dist = s2 * y;
+  r.ok = r.ok && fabs(fma(-dist, y, 1.)) <= 0x1p-50;
+  r.kx = dx * y;
+  r.ky = dy * y;
+  r.kz = dz * y;
+  r.dist = dist;
+  constexpr double kInverseC = 1. / kSpeedOfLight;
+  if (p.homogeneous > 0.) {
+    r.time = p.homogeneous * dist * kInverseC;
+    r.n_src = r.n_dst = p.homogeneous;
+    r.time_err = 0x1p-48 * fabs(r.time);
+    r.ok = r.ok && r.time_err < 1.e300;
+    return r;
+  }
+  double const sh = (sz - p.min_height) * p.inv_step;
+  double const dh = o.dest_height;
+  uint64_t const last = p.table_size - 1;
+  double n_src = 1., i_src = 1., n_dst = o.dest_n, height = 1.;
+  if (sh + 0.5 >= static_cast<double>(last)) {
+    double2 const t = __ldg(p.table + last);
+    n_src = t.x + p.slope_n_upper * fabs((sz - p.max_height) * p.inv_step) + 1.;
+    i_src = t.y + p.slope_i_upper * fabs(p.max_height - sz);
+    height = sh - dh;
+  } else if (sh + 0.5 < static_cast<double>(last) && sh > 0.) {
+    uint64_t const si = static_cast<uint64_t>(sh + 0.5);
+    double2 const t = __ldg(p.table + si);
+    n_src = t.x + 1.;
+    i_src = t.y;
+    height = static_cast<double>(static_cast<int64_t>(si) - static_cast<int64_t>(o.dest_index)) *
+             p.step;
+    if (height == 0.) height = 1.;
+  } else if (sh == 0.) {
+    n_src = 1.;
+    n_dst = 1.;
+    i_src = __ldg(p.table).y;
+    height = dh - sh;
+  } else {
+    double2 const t0 = __ldg(p.table);
+    n_src = t0.x + p.slope_n_lower * fabs(sh) + 1.;
+    i_src = t0.y + p.slope_i_lower * fabs(sh);
+    n_dst = 1.;
+    height = dh - fabs(sh);
+  }
+  r.time = (1. + (i_src - o.dest_integral) / height) * dist * kInverseC;
+  r.n_src = n_src;
+  r.n_dst = n_dst;
+  r.time_err = 0x1p-48 * fabs(r.time);
+  r.ok = r.ok && r.time_err < 1.e300;  // false for infinite or NaN times
+  return r;
+}
+
 // separate_same_bin_endpoints, RadioProjection.inl:303-336.
 __device__ __forceinline__ void separate_same_bin(double& start, double& end, double res,
                                                   bool signed_order) {

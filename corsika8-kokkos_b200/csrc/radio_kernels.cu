@@ -366,6 +366,16 @@ __device__ __noinline__ Counts coreas_pair_exact(Track const t, Propagation cons
   return c;
 }
 
+// The propagation of the filtered paths: propagate_fast when kFast, else the
+// exact propagate (time_err 0).
+template <bool kFast>
+__device__ __forceinline__ FastPath filtered_path(Propagation const& p, ObserverCache const& o,
+                                                  double x, double y, double z) {
+  if (kFast) return propagate_fast(p, o, x, y, z);
+  Path const e = propagate<true>(p, o, x, y, z);
+  return FastPath{e.time, e.n_src, e.n_dst, e.dist, e.kx, e.ky, e.kz, 0., true};
+}
+
 // The common CoREAS pair of the windowed kernel (RadioProjection.inl:339-409
 // without its near-Cherenkov branch).  Returns false, having deposited
 // nothing, when the pair needs the near-Cherenkov branch or (kFilter) an exact
@@ -627,9 +637,12 @@ struct StagedSegment {
 
 // accumulate_zhs_segment (RadioProjection.inl:412-480) with every decision of
 // zhs_segment<kRuns = true, kFilter>, its samples staged instead of
-// deposited.  Returns false, staging nothing, when the segment needs the
-// per-index binning or (kFilter) an exact evaluation, or when the trace has
-// 2^26 bins or more (staged counts then stay far inside 32 bits per warp).
+// deposited.  With kFilter the midpoint propagation is propagate_fast: its
+// directions (8u) stay inside the n beta.k bound, and its time error adds to
+// the detection-time bound e_d.  Returns false, staging nothing, when the
+// segment needs the per-index binning or (kFilter) an exact evaluation, or
+// when the trace has 2^26 bins or more (staged counts then stay far inside 32
+// bits per warp).
 template <bool kFilter, class Amp>
 __device__ __forceinline__ bool zhs_stage(double p1x, double p1y, double p1z, double p2x,
                                           double p2y, double p2z, double t1, double t2,
@@ -638,7 +651,8 @@ __device__ __forceinline__ bool zhs_stage(double p1x, double p1y, double p1z, do
                                           StagedSegment<Amp>& out) {
   if (!(o.bins_d < 67108864.0)) return false;
   double const mx = (p1x + p2x) * 0.5, my = (p1y + p2y) * 0.5, mz = (p1z + p2z) * 0.5;
-  Path const path = propagate<true, kFilter>(p, o, mx, my, mz);
+  FastPath const path = filtered_path<kFilter>(p, o, mx, my, mz);
+  if (kFilter && !path.ok) return false;
   double const bk = t.bx * path.kx + t.by * path.ky + t.bz * path.kz;
   double const nbk = path.n_src * bk;
   double const mt = (t1 + t2) * 0.5;
@@ -649,7 +663,8 @@ __device__ __forceinline__ bool zhs_stage(double p1x, double p1y, double p1z, do
     double const beta1 = fabs(t.bx) + fabs(t.by) + fabs(t.bz) + 1.;
     double const e_nbk = path.n_src * beta1 * 0x1p-47 + 0x1p-50;
     double const h = fabs(t1 - mt) + fabs(t2 - mt);
-    e_d = e_nbk * h + 0x1p-50 * (fabs(t1 + path.time) + fabs(t2 + path.time) + fabs(nbk) * h);
+    e_d = e_nbk * h + 0x1p-50 * (fabs(t1 + path.time) + fabs(t2 + path.time) + fabs(nbk) * h) +
+          path.time_err;
   }
   double sign = 1.;
   if (d1 > d2) {
