@@ -865,10 +865,10 @@ __device__ __noinline__ Counts zhs_pair_exact(Track const t, Propagation const& 
 //
 // kFilter: F is estimated in FP32 as sin^2(theta) K with
 // sin^2 = |beta x d|^2 / (|beta|^2 |d|^2) and K = 2 pi L^2 / (|d| lambda); its
-// distance from the reference's FP64 F is at most 1.7e-6 sqrt(K F) + 1e-6 F +
-// 1e-12 K (cross-product cancellation and the FP32 roundings; used with a 4x
-// margin), so an estimate surely below 1 decides "one segment" exactly as the
-// reference does.
+// distance from the reference's FP64 F is at most 1.7e-6 sqrt(K F) + 4e-6 F +
+// 1e-12 K (cross-product cancellation, the FP32 roundings and the approximate
+// reciprocals; used with margins of 2.3x and more), so an estimate surely
+// below 1 decides "one segment" exactly as the reference does.
 template <bool kFilter, class Amp>
 __device__ __forceinline__ bool zhs_common(Track const& t, Propagation const& p,
                                            ObserverCache const& o, Counts& c,
@@ -884,10 +884,14 @@ __device__ __forceinline__ bool zhs_common(Track const& t, Propagation const& p,
     float const d2 = dx * dx + dy * dy + dz * dz;
     float const b2 = bx * bx + by * by + bz * bz;
     float const length = static_cast<float>(t.length);
-    float const s2 = (cx * cx + cy * cy + cz * cz) / (b2 * d2);
-    float const k = 6.2831853f * length * length / (sqrtf(d2) * static_cast<float>(o.wavelength));
+    // approximate reciprocals and square roots (relative errors near 2^-21,
+    // inside the 4e-5 (f + 1) term below)
+    float const s2 = __fdividef(cx * cx + cy * cy + cz * cz, b2 * d2);
+    float const k = __fdividef(6.2831853f * length * length * rsqrtf(d2), static_cast<float>(o.wavelength));
     float const f = s2 * k;
-    float const margin = 4.e-6f * sqrtf(k * (f + 1.f)) + 4.e-5f * (f + 1.f) + 4.e-12f * k;
+    float const kf = k * (f + 1.f);
+    float const root = kf > 0.f ? kf * rsqrtf(kf) : 0.f;
+    float const margin = 4.e-6f * root + 4.e-5f * (f + 1.f) + 4.e-12f * k;
     if (!(f + margin < 1.f)) return false;
   } else {
     Path const pm = propagate<false>(p, o, mx, my, mz);
