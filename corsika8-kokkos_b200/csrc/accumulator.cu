@@ -600,7 +600,7 @@ class Accumulator {
 
   std::size_t device_bytes() const {
     std::size_t total = table_.bytes() + counters_.bytes() + slot_.bytes() + next_item_.bytes() +
-                        staging_.bytes() + staging2_.bytes() + tracks_.bytes();
+                        staging_.bytes() + staging2_.bytes() + tracks_.bytes() + deferred_.bytes();
     for (int a = 0; a < 2; ++a)
       total += observers_[a].bytes() + fixed_traces_[a].bytes() + float_traces_[a].bytes() +
                decoded_[a].bytes() + decode_offsets_[a].bytes() + decode_factors_[a].bytes();
@@ -828,6 +828,19 @@ class Accumulator {
     return ev;
   }
 
+  // The ZHS launch's per-CTA deferred lists, grown after the earlier work on
+  // stream_ (which the previous ZHS launch joined) when a launch needs more.
+  unsigned* deferred_lists(uint64_t entries) {
+    if (deferred_.count < entries) {
+      check(cudaStreamSynchronize(stream_), "deferred list fence");
+      DeviceBuffer<unsigned> fresh;
+      fresh.allocate(entries);
+      deferred_.swap(fresh);
+      stats_.device_bytes = device_bytes();
+    }
+    return deferred_.ptr;
+  }
+
   void project_direct(std::size_t count) {
     EventPlan const ev = make_event(count);
     bool const c = ev.observer_count[0] != 0, z = ev.observer_count[1] != 0;
@@ -884,6 +897,10 @@ class Accumulator {
       uint64_t ctas = static_cast<uint64_t>(per_sm) * sms_;
       append_work(plan, ev, ctas, true);
       if (ctas > plan.total_items) ctas = plan.total_items;
+      if (algorithm == 1) {
+        plan.deferred_stride = deferred_list_stride(plan);
+        plan.deferred = deferred_lists(ctas * plan.deferred_stride);
+      }
       check(cudaMemsetAsync(plan.next_item, 0, sizeof(unsigned), s), "memset");
       cudaEvent_t b = nullptr, e = nullptr;
       if (timing_) {
@@ -954,6 +971,7 @@ class Accumulator {
   DeviceBuffer<DeviceCounters> counters_;
   DeviceBuffer<unsigned long long> slot_;
   DeviceBuffer<unsigned> next_item_;
+  DeviceBuffer<unsigned> deferred_;  // the ZHS launch's per-CTA deferred lists
   DeviceBuffer<double> tracks_;
   std::size_t capacity_ = 0;
   std::size_t staged_ = 0;  // records ingested since the last projection (upper bound of tracks)
@@ -1143,6 +1161,10 @@ class Batch {
               append_work(l.plan, active[members[m]].second, ctas, m + 1 == members.size());
         uint64_t const items = l.plan.total_items;
         if (ctas > items) ctas = items;
+        if (algorithm == 1) {
+          l.plan.deferred_stride = deferred_list_stride(l.plan);
+          l.plan.deferred = deferred_lists(ctas * l.plan.deferred_stride);
+        }
         l.ctas = static_cast<int>(ctas);
         out.launches.push_back(l);
       }
@@ -1159,7 +1181,26 @@ class Batch {
   }
 
   cudaStream_t stream_ = nullptr;
+  // The ZHS launches' per-CTA deferred lists, grown after the batch stream's
+  // earlier work when a plan needs more; captured graphs that name the old
+  // lists are dropped.
+  unsigned* deferred_lists(uint64_t entries) {
+    if (deferred_.count < entries) {
+      check(cudaStreamSynchronize(stream_), "deferred list fence");
+      for (auto& g : graphs_) {
+        cudaGraphExecDestroy(g.second.exec);
+        cudaGraphDestroy(g.second.graph);
+      }
+      graphs_.clear();
+      DeviceBuffer<unsigned> fresh;
+      fresh.allocate(entries);
+      deferred_.swap(fresh);
+    }
+    return deferred_.ptr;
+  }
+
   DeviceBuffer<unsigned> next_item_;
+  DeviceBuffer<unsigned> deferred_;
   std::map<std::string, Graph> graphs_;
   uint64_t captures_ = 0;
 };

@@ -1,8 +1,9 @@
 // no_alloc.cu — c8r_accumulate_device_no_alloc: the record ingest and the
 // windowed projection with every piece of device scratch (packed track
-// kinematics, observer constants, refractivity table, valid-track slot, work
-// counter, fallback counters) in one file-scope static device array, so that
-// a call allocates no device memory.
+// kinematics, observer constants, refractivity table, the ZHS launch's
+// deferred-pair lists, valid-track slot, work counter, fallback counters) in
+// one file-scope static device array, so that a call allocates no device
+// memory.
 //
 // Who needs it: a transport code that has handed the whole of HBM to its own
 // pool (a Kokkos memory pool, a particle stack sized to the card) cannot get
@@ -51,10 +52,14 @@ constexpr std::size_t kSlotOffset = 512;
 constexpr std::size_t kNextItemOffset = 768;
 constexpr std::size_t kTableOffset = 1024;
 constexpr std::size_t kObserversOffset = kTableOffset + kMaxTableEntries * sizeof(double2);
-constexpr std::size_t kTracksOffset = kObserversOffset + kMaxObservers * sizeof(ObserverCache);
+// the ZHS launch's per-CTA deferred lists (track offsets of deferred pairs)
+constexpr std::size_t kDeferredOffset = kObserversOffset + kMaxObservers * sizeof(ObserverCache);
+constexpr std::size_t kDeferredEntries = std::size_t(2) << 20;
+constexpr std::size_t kTracksOffset = kDeferredOffset + kDeferredEntries * sizeof(unsigned);
 constexpr std::size_t kTrackCapacity = (kScratchBytes - kTracksOffset) / kTrackBytes;
 static_assert(sizeof(DeviceCounters) <= kSlotOffset - kCountersOffset, "scratch layout");
-static_assert(kObserversOffset % 256 == 0 && kTracksOffset % 256 == 0, "scratch alignment");
+static_assert(kObserversOffset % 256 == 0 && kDeferredOffset % 256 == 0 && kTracksOffset % 256 == 0,
+              "scratch alignment");
 static_assert(kTrackCapacity >= 65536, "scratch too small for a useful track chunk");
 
 constexpr int kMaxDevices = 64;
@@ -165,6 +170,7 @@ void accumulate_no_alloc(c8r_config const& config, c8r_lepton_transport_record c
   auto* const table = reinterpret_cast<double2*>(base + kTableOffset);
   auto* const caches = reinterpret_cast<ObserverCache*>(base + kObserversOffset);
   auto* const tracks = reinterpret_cast<double*>(base + kTracksOffset);
+  auto* const deferred = reinterpret_cast<unsigned*>(base + kDeferredOffset);
   DeviceCounters* const event_counters =
       counters ? reinterpret_cast<DeviceCounters*>(counters) : fallback_counters;
   if (!counters)
@@ -244,7 +250,10 @@ void accumulate_no_alloc(c8r_config const& config, c8r_lepton_transport_record c
     std::size_t const ctas_total = static_cast<std::size_t>(dev.sms) * 2;
     std::size_t const per_item = observers[0] + observers[1];
     std::size_t const target = std::max<std::size_t>(1, (16 * ctas_total + per_item - 1) / per_item);
-    std::size_t const chunk = std::max<std::size_t>(8192, (n + target - 1) / target);
+    // a chunk no longer than one CTA's share of the deferred lists
+    std::size_t const list_share = kDeferredEntries / (static_cast<std::size_t>(per_sm) * dev.sms);
+    std::size_t const chunk =
+        std::min(list_share, std::max<std::size_t>(8192, (n + target - 1) / target));
     ev.chunk_size = static_cast<uint32_t>(chunk);
     ev.chunks = static_cast<uint32_t>((n + chunk - 1) / chunk);
     for (int a = 0; a < 2; ++a) {
@@ -259,6 +268,8 @@ void accumulate_no_alloc(c8r_config const& config, c8r_lepton_transport_record c
       plan.next_item = next_item;
       uint64_t ctas = static_cast<uint64_t>(per_sm) * dev.sms;
       if (ctas > plan.total_items) ctas = plan.total_items;
+      plan.deferred = deferred;
+      plan.deferred_stride = static_cast<uint32_t>(chunk);
       check(cudaMemsetAsync(next_item, 0, sizeof(unsigned), stream), "radio scratch clear");
       check(c8r::launch_windowed(plan, fixed, precision, static_cast<int>(ctas), threads, stream),
             "radio windowed launch");

@@ -823,12 +823,17 @@ __device__ __forceinline__ void zhs_pair(Track const& t, Propagation const& p,
   // point2 = start + (end - start) / 1 / 1, exactly the reference's values.
   bool const subdivided = subtracks > 1 || refinement > 1;
   double rx = t.ex - t.sx, ry = t.ey - t.sy, rz = t.ez - t.sz, rt = t.te - t.ts;
-  if (subdivided) {  // x / 1 / 1 == x exactly, so undivided tracks skip the divisions
+  if (refinement > 1) {  // x / 1 == x exactly: undivided tracks skip the divisions
     double const rd = static_cast<double>(refinement);
     rx = rx / divisor / rd;
     ry = ry / divisor / rd;
     rz = rz / divisor / rd;
     rt = rt / divisor / rd;
+  } else if (subdivided) {
+    rx = rx / divisor;
+    ry = ry / divisor;
+    rz = rz / divisor;
+    rt = rt / divisor;
   }
   double p1x = t.sx, p1y = t.sy, p1z = t.sz, t1 = t.ts;
   // subtrack-major, refinement-minor order of the reference's nested loops
@@ -848,20 +853,11 @@ __device__ __forceinline__ void zhs_pair(Track const& t, Propagation const& p,
         static_cast<long long>(subtracks * (refinement - 1)));
 }
 
-// The exact pair out of line: deferred ZHS pairs of the windowed kernel.
-template <bool kFixed, class Amp, class Sink>
-__device__ __noinline__ Counts zhs_pair_exact(Track const t, Propagation const& p,
-                                              ObserverCache const& o, Sink sink) {
-  Counts c;
-  zhs_pair<kFixed, true, Amp>(t, p, o, sink, c, nullptr);
-  return c;
-}
-
 // The common ZHS pair of the windowed kernel: one undivided segment, staged
 // for the warp's cooperative deposit.  Returns false, staging nothing, when
 // the track is subdivided (Fraunhofer number above 1, or refinement), when
 // (kFilter) the Fraunhofer test is not surely below 1, or when zhs_stage
-// declines the segment; the kernel then defers the pair to zhs_pair_exact.
+// declines the segment; the kernel then defers the pair to zhs_drain.
 //
 // kFilter: F is estimated in FP32 as sin^2(theta) K with
 // sin^2 = |beta x d|^2 / (|beta|^2 |d|^2) and K = 2 pi L^2 / (|d| lambda); its
@@ -1203,6 +1199,108 @@ __device__ __forceinline__ uint32_t find_event(EventPlan const* events, uint32_t
   return lo;
 }
 
+// Deferred ZHS pairs of the windowed kernel, drained by the whole warp
+// (accumulate_zhs, RadioProjection.inl:483-529).  Lanes below `count` take
+// one deferred pair each and evaluate its Fraunhofer number and subdivision
+// exactly; the warp then steps through segment index s = 0, 1, ...: every lane
+// whose pair has a segment s forms its endpoints by the reference's
+// sequential additions, stages it (kFilter: the filtered decisions first, the
+// exact ones where those are ambiguous), and the warp deposits the staged
+// samples together.  A segment that needs the per-index binning deposits on
+// its own lane.  Every lane of the warp calls it.
+template <bool kFixed, bool kFilter, class Amp, class Sink>
+__device__ __noinline__ Counts zhs_drain(const double* __restrict__ tracks, uint64_t begin,
+                                         unsigned const* queue, unsigned count,
+                                         Propagation const& p, ObserverCache const& o, Sink sink,
+                                         StagedSegment<Amp>* staging) {
+  Counts c;
+  unsigned const lane = threadIdx.x & 31u;
+  uint64_t row = 0;
+  long long segments = 0;
+  bool subdivided = false;
+  double p1x = 0., p1y = 0., p1z = 0., t1 = 0., rx = 0., ry = 0., rz = 0., rt = 0.;
+  if (lane < count) {
+    row = begin + queue[lane];
+    Track const t = load_track(tracks, 0, row);
+    double const mx = (t.sx + t.ex) * 0.5, my = (t.sy + t.ey) * 0.5, mz = (t.sz + t.ez) * 0.5;
+    Path const pm = propagate<false>(p, o, mx, my, mz);
+    double const uk = (t.bx * pm.kx + t.by * pm.ky + t.bz * pm.kz) / t.beta_module;
+    double const s2 = 1. - uk * uk;
+    double const fraunhofer = s2 * t.length * t.length / pm.dist / o.wavelength * 2. * kPi;
+    double divisor = 1.;
+    int subtracks = 1;
+    if (fraunhofer > 1.) {
+      divisor = sqrt(fraunhofer) + 1.;
+      subtracks = x86_int(ceil(divisor));
+    }
+    int const refinement = static_cast<int>(p.refinement);
+    c.subtracks += static_cast<unsigned long long>(static_cast<long long>(subtracks));
+    if (refinement > 1)
+      c.subtracks += static_cast<unsigned long long>(
+          static_cast<long long>(subtracks * (refinement - 1)));
+    subdivided = subtracks > 1 || refinement > 1;
+    rx = t.ex - t.sx;
+    ry = t.ey - t.sy;
+    rz = t.ez - t.sz;
+    rt = t.te - t.ts;
+    if (refinement > 1) {  // x / 1 == x exactly: undivided tracks skip the divisions
+      double const rd = static_cast<double>(refinement);
+      rx = rx / divisor / rd;
+      ry = ry / divisor / rd;
+      rz = rz / divisor / rd;
+      rt = rt / divisor / rd;
+    } else if (subdivided) {
+      rx = rx / divisor;
+      ry = ry / divisor;
+      rz = rz / divisor;
+      rt = rt / divisor;
+    }
+    segments = static_cast<long long>(subtracks) * refinement;
+    p1x = t.sx;
+    p1y = t.sy;
+    p1z = t.sz;
+    t1 = t.ts;
+  }
+#pragma unroll 1
+  for (long long s = 0; __any_sync(0xffffffffu, s < segments); ++s) {
+    StagedSegment<Amp> seg;
+    seg.count = 0u;
+    seg.flags = 0u;
+    if (s < segments) {
+      // velocity and charge constant read again each step (L1): fewer
+      // registers held across the warp's steps
+      double2 const* r = reinterpret_cast<double2 const*>(tracks + row * kTrackDoubles);
+      asm volatile("" : "+l"(r));
+      double2 const e = __ldg(r + 4), f = __ldg(r + 5), g = __ldg(r + 6);
+      Track t;
+      t.bx = e.x;
+      t.by = e.y;
+      t.bz = f.x;
+      t.length = f.y;
+      t.beta_module = g.x;
+      t.constant = g.y;
+      double const p2x = p1x + rx, p2y = p1y + ry, p2z = p1z + rz, t2 = t1 + rt;
+      bool staged =
+          zhs_stage<kFilter, Amp>(p1x, p1y, p1z, p2x, p2y, p2z, t1, t2, t, p, o, subdivided, seg);
+      if (kFilter && !staged)
+        staged = zhs_stage<false, Amp>(p1x, p1y, p1z, p2x, p2y, p2z, t1, t2, t, p, o, subdivided,
+                                       seg);
+      if (!staged) {
+        seg.count = 0u;
+        seg.flags = 0u;
+        zhs_segment<kFixed, true, false, Amp>(p1x, p1y, p1z, p2x, p2y, p2z, t1, t2, t, p, o, sink,
+                                              c, subdivided, nullptr);
+      }
+      p1x = p2x;
+      p1y = p2y;
+      p1z = p2z;
+      t1 = t2;
+    }
+    deposit_staged<kFixed>(staging, seg, o, sink, c);
+  }
+  return c;
+}
+
 template <bool kFixed, class Amp, int kAlgorithm>
 __global__ void __launch_bounds__(kAlgorithm == 1 ? kZhsThreadsMax : kWindowThreadsMax, 1)
     windowed_kernel(const __grid_constant__ WorkPlan plan) {
@@ -1210,6 +1308,11 @@ __global__ void __launch_bounds__(kAlgorithm == 1 ? kZhsThreadsMax : kWindowThre
   __shared__ unsigned long long item_shared;
   __shared__ ObserverCache observer;
   __shared__ float window_bound;
+  __shared__ unsigned deferred_total;
+  // ZHS: this CTA's list of the deferred pairs of its current item
+  unsigned* const deferred_list =
+      kAlgorithm == 1 ? plan.deferred + static_cast<size_t>(blockIdx.x) * plan.deferred_stride
+                      : nullptr;
   Counts c;
   for (;;) {
     __syncthreads();
@@ -1248,10 +1351,13 @@ __global__ void __launch_bounds__(kAlgorithm == 1 ? kZhsThreadsMax : kWindowThre
       sink.frow[row] = kFixed ? nullptr : ev.floating[algorithm] + row * total + o.offset;
     }
     constexpr bool kFilter = sizeof(Amp) == sizeof(float);  // mixed precision
-    // Per-warp queue of deferred pairs (track offsets in the chunk): pairs that
-    // need the near-Cherenkov branch, an exact evaluation or a subdivided
-    // track.  A warp drains 32 of them at a time, converged, with the exact
-    // code, so rare paths do not hold up the common path of the other lanes.
+    // Deferred pairs (track offsets in the chunk) leave the common path, so
+    // rare paths do not hold up the other lanes.  CoREAS (the near-Cherenkov
+    // branch, exact evaluations): a per-warp queue in shared memory, drained
+    // 32 at a time, converged, with the exact code.  ZHS (subdivided tracks,
+    // exact evaluations): the CTA's list in global memory, drained by all
+    // warps after the item's tracks (zhs_drain), which keeps every call out of
+    // the track loop.
     unsigned* const queue =
         reinterpret_cast<unsigned*>(window + 3 * static_cast<size_t>(plan.window)) +
         (threadIdx.x >> 5) * kWarpQueue;
@@ -1267,8 +1373,7 @@ __global__ void __launch_bounds__(kAlgorithm == 1 ? kZhsThreadsMax : kWindowThre
     auto drain = [&](unsigned from, unsigned count) {
       if (lane < count) {
         Track const t = load_track(ev.tracks, ev.stride, begin + queue[from + lane]);
-        Counts const d = kAlgorithm == 0 ? coreas_pair_exact<kFixed, Amp>(t, ev.propagation, o, sink)
-                                         : zhs_pair_exact<kFixed, Amp>(t, ev.propagation, o, sink);
+        Counts const d = coreas_pair_exact<kFixed, Amp>(t, ev.propagation, o, sink);
         c.coreas += d.coreas;
         c.zhs += d.zhs;
         c.subtracks += d.subtracks;
@@ -1292,6 +1397,10 @@ __global__ void __launch_bounds__(kAlgorithm == 1 ? kZhsThreadsMax : kWindowThre
       sink.unchecked = kFixed && attempt == 0 && bins <= width;
       c.mag = 0.f;
       queued = 0;
+      if (kAlgorithm == 1) {
+        if (threadIdx.x == 0) deferred_total = 0u;
+        __syncthreads();
+      }
       for (uint64_t base = begin; base < end; base += blockDim.x) {
         uint64_t const i = base + threadIdx.x;
         bool deferred = false;
@@ -1307,16 +1416,38 @@ __global__ void __launch_bounds__(kAlgorithm == 1 ? kZhsThreadsMax : kWindowThre
         }
         if (kAlgorithm == 1) deposit_staged<kFixed>(staging, seg, o, sink, c);
         unsigned const ballot = __ballot_sync(0xffffffffu, deferred);
-        if (deferred)
-          queue[queued + __popc(ballot & ((1u << lane) - 1u))] = static_cast<unsigned>(i - begin);
-        queued += __popc(ballot);
-        __syncwarp();
-        if (queued >= 32u) {
-          queued -= 32u;
-          drain(queued, 32u);
+        unsigned const rank = __popc(ballot & ((1u << lane) - 1u));
+        if (kAlgorithm == 1) {
+          if (ballot) {
+            unsigned slot = 0;
+            if (lane == 0) slot = atomicAdd(&deferred_total, static_cast<unsigned>(__popc(ballot)));
+            slot = __shfl_sync(0xffffffffu, slot, 0);
+            if (deferred) deferred_list[slot + rank] = static_cast<unsigned>(i - begin);
+          }
+        } else {
+          if (deferred) queue[queued + rank] = static_cast<unsigned>(i - begin);
+          queued += __popc(ballot);
+          __syncwarp();
+          if (queued >= 32u) {
+            queued -= 32u;
+            drain(queued, 32u);
+          }
         }
       }
-      if (queued) drain(0u, queued);
+      if (kAlgorithm == 0 && queued) drain(0u, queued);
+      if (kAlgorithm == 1) {
+        __syncthreads();
+        unsigned const n = deferred_total;  // at most end - begin <= deferred_stride
+        for (unsigned from = (threadIdx.x >> 5) * 32u; from < n; from += (blockDim.x >> 5) * 32u) {
+          Counts const d = zhs_drain<kFixed, kFilter, Amp>(ev.tracks, begin, deferred_list + from,
+                                                           n - from < 32u ? n - from : 32u,
+                                                           ev.propagation, o, sink, staging);
+          c.zhs += d.zhs;
+          c.subtracks += d.subtracks;
+          c.overflows += d.overflows;
+          c.mag += d.mag;
+        }
+      }
       __syncthreads();
       if (!sink.unchecked) break;
       float const thread_bound = static_cast<float>(warp_sum(static_cast<double>(c.mag)));
@@ -1425,6 +1556,8 @@ size_t windowed_smem_bytes(uint32_t window, int algorithm) {
 template <bool kFixed, class Amp, int kAlgorithm>
 cudaError_t windowed_dispatch_algorithm(WorkPlan const& plan, int ctas, int threads,
                                         cudaStream_t stream) {
+  if (kAlgorithm == 1 && (plan.deferred == nullptr || plan.deferred_stride < deferred_list_stride(plan)))
+    return cudaErrorInvalidValue;
   size_t const bytes = windowed_smem_bytes(plan.window, kAlgorithm);
   cudaError_t err = cudaFuncSetAttribute(windowed_kernel<kFixed, Amp, kAlgorithm>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -234,6 +234,7 @@ class Server {
     cudaStreamDestroy(admit_);
     cudaStreamDestroy(fetch_);
     cudaFree(next_item_);
+    if (deferred_) cudaFree(deferred_);
     arena_.free_all();
     if (previous >= 0) cudaSetDevice(previous);
   }
@@ -690,6 +691,19 @@ class Server {
     return per_sm;
   }
 
+  // Grown after the rounds in flight on compute_ when a launch needs more.
+  unsigned* deferred_lists(uint64_t entries) {
+    if (deferred_entries_ < entries) {
+      check(cudaStreamSynchronize(compute_), "deferred list fence");
+      if (deferred_) cudaFree(deferred_);
+      deferred_ = nullptr;
+      deferred_entries_ = 0;
+      check(cudaMalloc(&deferred_, entries * sizeof(unsigned)), "deferred lists");
+      deferred_entries_ = entries;
+    }
+    return deferred_;
+  }
+
   void launch(std::vector<Slice> const& slices) {
     uint64_t const id = ++launched_rounds_;
     for (Slice const& s : slices) {
@@ -741,6 +755,10 @@ class Server {
           append_work(plan, members[m], ctas, m + 1 == members.size());
         uint64_t const items = plan.total_items;
         if (ctas > items) ctas = items;
+        if (a == 1) {
+          plan.deferred_stride = deferred_list_stride(plan);
+          plan.deferred = deferred_lists(ctas * plan.deferred_stride);
+        }
         check(cudaMemsetAsync(counter, 0, sizeof(unsigned), compute_), "server work counter");
         check(launch_windowed(plan, fixed, precision, static_cast<int>(ctas), threads_, compute_),
               "server windowed launch");
@@ -773,6 +791,8 @@ class Server {
   Arena arena_;
   cudaStream_t compute_ = nullptr, admit_ = nullptr, fetch_ = nullptr;
   unsigned* next_item_ = nullptr;
+  unsigned* deferred_ = nullptr;  // the ZHS launches' per-CTA deferred lists
+  uint64_t deferred_entries_ = 0;
   std::chrono::steady_clock::time_point epoch_;
   std::mutex mu_, fetch_mu_;
   std::condition_variable work_cv_, memory_cv_, done_cv_;
