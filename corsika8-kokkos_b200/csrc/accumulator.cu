@@ -600,7 +600,8 @@ class Accumulator {
 
   std::size_t device_bytes() const {
     std::size_t total = table_.bytes() + counters_.bytes() + slot_.bytes() + next_item_.bytes() +
-                        staging_.bytes() + staging2_.bytes() + tracks_.bytes() + deferred_.bytes();
+                        staging_.bytes() + staging2_.bytes() + tracks_.bytes() + deferred_[0].bytes() +
+                        deferred_[1].bytes();
     for (int a = 0; a < 2; ++a)
       total += observers_[a].bytes() + fixed_traces_[a].bytes() + float_traces_[a].bytes() +
                decoded_[a].bytes() + decode_offsets_[a].bytes() + decode_factors_[a].bytes();
@@ -828,17 +829,19 @@ class Accumulator {
     return ev;
   }
 
-  // The ZHS launch's per-CTA deferred lists, grown after the earlier work on
-  // stream_ (which the previous ZHS launch joined) when a launch needs more.
-  unsigned* deferred_lists(uint64_t entries) {
-    if (deferred_.count < entries) {
+  // Per-CTA deferred-pair lists of each algorithm's launch (the two launches
+  // may run side by side), grown after the earlier work on stream_ (which the
+  // previous ZHS launch joined) when a launch needs more.
+  unsigned* deferred_lists(int algorithm, uint64_t entries) {
+    DeviceBuffer<unsigned>& lists = deferred_[algorithm];
+    if (lists.count < entries) {
       check(cudaStreamSynchronize(stream_), "deferred list fence");
       DeviceBuffer<unsigned> fresh;
       fresh.allocate(entries);
-      deferred_.swap(fresh);
+      lists.swap(fresh);
       stats_.device_bytes = device_bytes();
     }
-    return deferred_.ptr;
+    return lists.ptr;
   }
 
   void project_direct(std::size_t count) {
@@ -897,10 +900,8 @@ class Accumulator {
       uint64_t ctas = static_cast<uint64_t>(per_sm) * sms_;
       append_work(plan, ev, ctas, true);
       if (ctas > plan.total_items) ctas = plan.total_items;
-      if (algorithm == 1) {
-        plan.deferred_stride = deferred_list_stride(plan);
-        plan.deferred = deferred_lists(ctas * plan.deferred_stride);
-      }
+      plan.deferred_stride = deferred_list_stride(plan);
+      plan.deferred = deferred_lists(algorithm, ctas * plan.deferred_stride);
       check(cudaMemsetAsync(plan.next_item, 0, sizeof(unsigned), s), "memset");
       cudaEvent_t b = nullptr, e = nullptr;
       if (timing_) {
@@ -971,7 +972,7 @@ class Accumulator {
   DeviceBuffer<DeviceCounters> counters_;
   DeviceBuffer<unsigned long long> slot_;
   DeviceBuffer<unsigned> next_item_;
-  DeviceBuffer<unsigned> deferred_;  // the ZHS launch's per-CTA deferred lists
+  DeviceBuffer<unsigned> deferred_[2];  // per-CTA deferred-pair lists, by algorithm
   DeviceBuffer<double> tracks_;
   std::size_t capacity_ = 0;
   std::size_t staged_ = 0;  // records ingested since the last projection (upper bound of tracks)
@@ -1161,10 +1162,8 @@ class Batch {
               append_work(l.plan, active[members[m]].second, ctas, m + 1 == members.size());
         uint64_t const items = l.plan.total_items;
         if (ctas > items) ctas = items;
-        if (algorithm == 1) {
-          l.plan.deferred_stride = deferred_list_stride(l.plan);
-          l.plan.deferred = deferred_lists(ctas * l.plan.deferred_stride);
-        }
+        l.plan.deferred_stride = deferred_list_stride(l.plan);
+        l.plan.deferred = deferred_lists(ctas * l.plan.deferred_stride);
         l.ctas = static_cast<int>(ctas);
         out.launches.push_back(l);
       }
@@ -1181,9 +1180,9 @@ class Batch {
   }
 
   cudaStream_t stream_ = nullptr;
-  // The ZHS launches' per-CTA deferred lists, grown after the batch stream's
-  // earlier work when a plan needs more; captured graphs that name the old
-  // lists are dropped.
+  // The launches' per-CTA deferred-pair lists (the launches run one after the
+  // other), grown after the batch stream's earlier work when a plan needs
+  // more; captured graphs that name the old lists are dropped.
   unsigned* deferred_lists(uint64_t entries) {
     if (deferred_.count < entries) {
       check(cudaStreamSynchronize(stream_), "deferred list fence");

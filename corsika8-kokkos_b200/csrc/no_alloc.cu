@@ -1,6 +1,6 @@
 // no_alloc.cu — c8r_accumulate_device_no_alloc: the record ingest and the
 // windowed projection with every piece of device scratch (packed track
-// kinematics, observer constants, refractivity table, the ZHS launch's
+// kinematics, observer constants, refractivity table, the launches'
 // deferred-pair lists, valid-track slot, work counter, fallback counters) in
 // one file-scope static device array, so that a call allocates no device
 // memory.
@@ -52,7 +52,7 @@ constexpr std::size_t kSlotOffset = 512;
 constexpr std::size_t kNextItemOffset = 768;
 constexpr std::size_t kTableOffset = 1024;
 constexpr std::size_t kObserversOffset = kTableOffset + kMaxTableEntries * sizeof(double2);
-// the ZHS launch's per-CTA deferred lists (track offsets of deferred pairs)
+// the launches' per-CTA deferred-pair lists (track offsets in the chunk)
 constexpr std::size_t kDeferredOffset = kObserversOffset + kMaxObservers * sizeof(ObserverCache);
 constexpr std::size_t kDeferredEntries = std::size_t(2) << 20;
 constexpr std::size_t kTracksOffset = kDeferredOffset + kDeferredEntries * sizeof(unsigned);

@@ -1182,8 +1182,6 @@ constexpr int kWindowThreadsMax = kWindowThreads;
 // The ZHS kernel's live state needs more than 128 registers a thread: it runs
 // 384-thread CTAs (up to 168 registers, no spills).
 constexpr int kZhsThreadsMax = 384;
-constexpr unsigned kWarpQueue = 64;  // entries per warp: < 32 kept + 32 pushed per round
-constexpr size_t kQueueBytes = (kWindowThreadsMax / 32) * kWarpQueue * sizeof(unsigned);
 // staging slots of the ZHS kernel: 32 per warp, sized for the FP64 amplitudes
 constexpr size_t kStagingBytes = (kZhsThreadsMax / 32) * 32 * sizeof(StagedSegment<double>);
 
@@ -1210,7 +1208,7 @@ __device__ __forceinline__ uint32_t find_event(EventPlan const* events, uint32_t
 // its own lane.  Every lane of the warp calls it.
 template <bool kFixed, bool kFilter, class Amp, class Sink>
 __device__ __noinline__ Counts zhs_drain(const double* __restrict__ tracks, uint64_t begin,
-                                         unsigned const* queue, unsigned count,
+                                         unsigned const* list, unsigned count,
                                          Propagation const& p, ObserverCache const& o, Sink sink,
                                          StagedSegment<Amp>* staging) {
   Counts c;
@@ -1220,7 +1218,7 @@ __device__ __noinline__ Counts zhs_drain(const double* __restrict__ tracks, uint
   bool subdivided = false;
   double p1x = 0., p1y = 0., p1z = 0., t1 = 0., rx = 0., ry = 0., rz = 0., rt = 0.;
   if (lane < count) {
-    row = begin + queue[lane];
+    row = begin + list[lane];
     Track const t = load_track(tracks, 0, row);
     double const mx = (t.sx + t.ex) * 0.5, my = (t.sy + t.ey) * 0.5, mz = (t.sz + t.ez) * 0.5;
     Path const pm = propagate<false>(p, o, mx, my, mz);
@@ -1310,9 +1308,7 @@ __global__ void __launch_bounds__(kAlgorithm == 1 ? kZhsThreadsMax : kWindowThre
   __shared__ float window_bound;
   __shared__ unsigned deferred_total;
   // ZHS: this CTA's list of the deferred pairs of its current item
-  unsigned* const deferred_list =
-      kAlgorithm == 1 ? plan.deferred + static_cast<size_t>(blockIdx.x) * plan.deferred_stride
-                      : nullptr;
+  unsigned* const deferred_list = plan.deferred + static_cast<size_t>(blockIdx.x) * plan.deferred_stride;
   Counts c;
   for (;;) {
     __syncthreads();
@@ -1351,37 +1347,18 @@ __global__ void __launch_bounds__(kAlgorithm == 1 ? kZhsThreadsMax : kWindowThre
       sink.frow[row] = kFixed ? nullptr : ev.floating[algorithm] + row * total + o.offset;
     }
     constexpr bool kFilter = sizeof(Amp) == sizeof(float);  // mixed precision
-    // Deferred pairs (track offsets in the chunk) leave the common path, so
-    // rare paths do not hold up the other lanes.  CoREAS (the near-Cherenkov
-    // branch, exact evaluations): a per-warp queue in shared memory, drained
-    // 32 at a time, converged, with the exact code.  ZHS (subdivided tracks,
-    // exact evaluations): the CTA's list in global memory, drained by all
-    // warps after the item's tracks (zhs_drain), which keeps every call out of
-    // the track loop.
-    unsigned* const queue =
-        reinterpret_cast<unsigned*>(window + 3 * static_cast<size_t>(plan.window)) +
-        (threadIdx.x >> 5) * kWarpQueue;
+    // Deferred pairs (track offsets in the chunk: CoREAS pairs for the
+    // near-Cherenkov branch or an exact evaluation, ZHS pairs with subdivided
+    // tracks or an exact evaluation) leave the common path, so rare paths do
+    // not hold up the other lanes: they go to the CTA's list in global memory
+    // and all warps drain it, 32 pairs at a time, after the item's tracks.
+    // The track loop then holds no call, which keeps its registers free.
     // per-warp staging slots of the ZHS kernel's cooperative deposit
     StagedSegment<Amp>* const staging =
-        reinterpret_cast<StagedSegment<Amp>*>(
-            reinterpret_cast<unsigned char*>(window + 3 * static_cast<size_t>(plan.window)) +
-            kQueueBytes) +
+        reinterpret_cast<StagedSegment<Amp>*>(window + 3 * static_cast<size_t>(plan.window)) +
         (threadIdx.x >> 5) * 32u;
     unsigned const lane = threadIdx.x & 31u;
-    unsigned queued = 0;  // warp-uniform
     Counts const saved = c;
-    auto drain = [&](unsigned from, unsigned count) {
-      if (lane < count) {
-        Track const t = load_track(ev.tracks, ev.stride, begin + queue[from + lane]);
-        Counts const d = coreas_pair_exact<kFixed, Amp>(t, ev.propagation, o, sink);
-        c.coreas += d.coreas;
-        c.zhs += d.zhs;
-        c.subtracks += d.subtracks;
-        c.overflows += d.overflows;
-        c.mag += d.mag;
-      }
-      __syncwarp();
-    };
     // Fixed point, whole trace in the window: the window takes unchecked
     // adds, and `c.mag` bounds the sum of |increments| of this thread.  If the
     // block's bound stays below 2^61 (the FP32 sums are off by a factor below
@@ -1396,11 +1373,8 @@ __global__ void __launch_bounds__(kAlgorithm == 1 ? kZhsThreadsMax : kWindowThre
       }
       sink.unchecked = kFixed && attempt == 0 && bins <= width;
       c.mag = 0.f;
-      queued = 0;
-      if (kAlgorithm == 1) {
-        if (threadIdx.x == 0) deferred_total = 0u;
-        __syncthreads();
-      }
+      if (threadIdx.x == 0) deferred_total = 0u;
+      __syncthreads();
       for (uint64_t base = begin; base < end; base += blockDim.x) {
         uint64_t const i = base + threadIdx.x;
         bool deferred = false;
@@ -1417,36 +1391,31 @@ __global__ void __launch_bounds__(kAlgorithm == 1 ? kZhsThreadsMax : kWindowThre
         if (kAlgorithm == 1) deposit_staged<kFixed>(staging, seg, o, sink, c);
         unsigned const ballot = __ballot_sync(0xffffffffu, deferred);
         unsigned const rank = __popc(ballot & ((1u << lane) - 1u));
-        if (kAlgorithm == 1) {
-          if (ballot) {
-            unsigned slot = 0;
-            if (lane == 0) slot = atomicAdd(&deferred_total, static_cast<unsigned>(__popc(ballot)));
-            slot = __shfl_sync(0xffffffffu, slot, 0);
-            if (deferred) deferred_list[slot + rank] = static_cast<unsigned>(i - begin);
-          }
-        } else {
-          if (deferred) queue[queued + rank] = static_cast<unsigned>(i - begin);
-          queued += __popc(ballot);
-          __syncwarp();
-          if (queued >= 32u) {
-            queued -= 32u;
-            drain(queued, 32u);
-          }
+        if (ballot) {
+          unsigned slot = 0;
+          if (lane == 0) slot = atomicAdd(&deferred_total, static_cast<unsigned>(__popc(ballot)));
+          slot = __shfl_sync(0xffffffffu, slot, 0);
+          if (deferred) deferred_list[slot + rank] = static_cast<unsigned>(i - begin);
         }
       }
-      if (kAlgorithm == 0 && queued) drain(0u, queued);
-      if (kAlgorithm == 1) {
-        __syncthreads();
-        unsigned const n = deferred_total;  // at most end - begin <= deferred_stride
-        for (unsigned from = (threadIdx.x >> 5) * 32u; from < n; from += (blockDim.x >> 5) * 32u) {
-          Counts const d = zhs_drain<kFixed, kFilter, Amp>(ev.tracks, begin, deferred_list + from,
-                                                           n - from < 32u ? n - from : 32u,
-                                                           ev.propagation, o, sink, staging);
-          c.zhs += d.zhs;
-          c.subtracks += d.subtracks;
-          c.overflows += d.overflows;
-          c.mag += d.mag;
+      __syncthreads();
+      unsigned const n = deferred_total;  // at most end - begin <= deferred_stride
+      for (unsigned from = (threadIdx.x >> 5) * 32u; from < n; from += (blockDim.x >> 5) * 32u) {
+        unsigned const count = n - from < 32u ? n - from : 32u;
+        Counts d;
+        if (kAlgorithm == 1) {
+          d = zhs_drain<kFixed, kFilter, Amp>(ev.tracks, begin, deferred_list + from, count,
+                                              ev.propagation, o, sink, staging);
+        } else if (lane < count) {
+          Track const t = load_track(ev.tracks, ev.stride, begin + deferred_list[from + lane]);
+          d = coreas_pair_exact<kFixed, Amp>(t, ev.propagation, o, sink);
         }
+        c.coreas += d.coreas;
+        c.zhs += d.zhs;
+        c.subtracks += d.subtracks;
+        c.overflows += d.overflows;
+        c.mag += d.mag;
+        __syncwarp();
       }
       __syncthreads();
       if (!sink.unchecked) break;
@@ -1547,16 +1516,16 @@ cudaError_t direct_dispatch(EventPlan const& ev, uint64_t bound, bool coreas, bo
   return cudaGetLastError();
 }
 
-// window rows | per-warp deferral queues | (ZHS) per-warp staging slots
+// window rows | (ZHS) per-warp staging slots
 size_t windowed_smem_bytes(uint32_t window, int algorithm) {
-  return static_cast<size_t>(window) * 3 * sizeof(unsigned long long) + kQueueBytes +
+  return static_cast<size_t>(window) * 3 * sizeof(unsigned long long) +
          (algorithm == 1 ? kStagingBytes : 0);
 }
 
 template <bool kFixed, class Amp, int kAlgorithm>
 cudaError_t windowed_dispatch_algorithm(WorkPlan const& plan, int ctas, int threads,
                                         cudaStream_t stream) {
-  if (kAlgorithm == 1 && (plan.deferred == nullptr || plan.deferred_stride < deferred_list_stride(plan)))
+  if (plan.deferred == nullptr || plan.deferred_stride < deferred_list_stride(plan))
     return cudaErrorInvalidValue;
   size_t const bytes = windowed_smem_bytes(plan.window, kAlgorithm);
   cudaError_t err = cudaFuncSetAttribute(windowed_kernel<kFixed, Amp, kAlgorithm>,
@@ -1639,7 +1608,7 @@ int windowed_max_bins(int device) {
   int optin = 0;
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
   // static shared memory of the kernel is a few hundred bytes; keep 1 KiB spare
-  int const usable = optin - 1024 - static_cast<int>(kQueueBytes + kStagingBytes);
+  int const usable = optin - 1024 - static_cast<int>(kStagingBytes);
   return usable > 0 ? usable / static_cast<int>(3 * sizeof(unsigned long long)) : 0;
 }
 

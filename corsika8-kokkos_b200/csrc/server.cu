@@ -755,10 +755,8 @@ class Server {
           append_work(plan, members[m], ctas, m + 1 == members.size());
         uint64_t const items = plan.total_items;
         if (ctas > items) ctas = items;
-        if (a == 1) {
-          plan.deferred_stride = deferred_list_stride(plan);
-          plan.deferred = deferred_lists(ctas * plan.deferred_stride);
-        }
+        plan.deferred_stride = deferred_list_stride(plan);
+        plan.deferred = deferred_lists(ctas * plan.deferred_stride);
         check(cudaMemsetAsync(counter, 0, sizeof(unsigned), compute_), "server work counter");
         check(launch_windowed(plan, fixed, precision, static_cast<int>(ctas), threads_, compute_),
               "server windowed launch");
@@ -791,7 +789,7 @@ class Server {
   Arena arena_;
   cudaStream_t compute_ = nullptr, admit_ = nullptr, fetch_ = nullptr;
   unsigned* next_item_ = nullptr;
-  unsigned* deferred_ = nullptr;  // the ZHS launches' per-CTA deferred lists
+  unsigned* deferred_ = nullptr;  // the launches' per-CTA deferred-pair lists
   uint64_t deferred_entries_ = 0;
   std::chrono::steady_clock::time_point epoch_;
   std::mutex mu_, fetch_mu_;

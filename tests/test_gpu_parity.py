@@ -327,9 +327,11 @@ def test_traces_longer_than_the_window(pkg, oracle, showers, torch_cuda, precisi
     got = gpu_project(pkg, torch_cuda, count_cfg, records)
     want = oracle.restatement().project(showers.make_config(wl, count_samples=True), records, threads=8)
     assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
-    # the window holds about 8400 bins on a B200 (227 KB of shared memory a block)
-    tail = got[0][0].reshape(8, 20000)[:, 8420:].sum() + got[1][0].reshape(8, 20000)[:, 8420:].sum()
-    head = got[0][0].reshape(8, 20000)[:, :8400].sum() + got[1][0].reshape(8, 20000)[:, :8400].sum()
+    # the window holds about 8600 bins on a B200 (227 KB of shared memory a block)
+    width = got[3].observer_tile_size
+    assert 8000 < width < 20000
+    tail = got[0][0].reshape(8, 20000)[:, width:].sum() + got[1][0].reshape(8, 20000)[:, width:].sum()
+    head = got[0][0].reshape(8, 20000)[:, :width].sum() + got[1][0].reshape(8, 20000)[:, :width].sum()
     assert tail > 0 and head > 0  # samples on both sides of the window edge
     if precision == 0:
         config = showers.make_config(wl, precision=0, kernel=2)
