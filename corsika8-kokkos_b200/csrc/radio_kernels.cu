@@ -747,8 +747,9 @@ __device__ __forceinline__ bool zhs_stage(double p1x, double p1y, double p1z, do
   return true;
 }
 
-// Deposits the staged segments of a warp: every lane takes one bin of the
-// flattened list (lane order, then bin order) per step.  Every lane of the
+// Deposits the staged segments of a warp: every lane takes two bins of the
+// flattened list (lane order, then bin order) per step, their owner searches
+// interleaved.  Every lane of the
 // warp calls it; `staging` is the warp's 32 slots in shared memory.
 template <bool kFixed, class Amp, class Sink>
 __device__ __forceinline__ void deposit_staged(StagedSegment<Amp>* staging,
@@ -773,29 +774,38 @@ __device__ __forceinline__ void deposit_staged(StagedSegment<Amp>* staging,
   grid.fixed_scale = o.fixed_scale;
   grid.fixed_scale_f = o.fixed_scale_f;
   grid.count_samples = o.count_samples;
-  for (uint32_t base = 0; base < total; base += 32u) {
-    uint32_t const j = base + lane;
-    uint32_t owner = 0;
+  for (uint32_t base = 0; base < total; base += 64u) {
+    uint32_t const j0 = base + lane, j1 = j0 + 32u;
+    uint32_t owner0 = 0, owner1 = 0;
 #pragma unroll
     for (uint32_t step = 16; step >= 1u; step >>= 1) {
-      uint32_t const v = __shfl_sync(0xffffffffu, incl, owner + step - 1u);
-      if (v <= j) owner += step;
+      uint32_t const v0 = __shfl_sync(0xffffffffu, incl, owner0 + step - 1u);
+      uint32_t const v1 = __shfl_sync(0xffffffffu, incl, owner1 + step - 1u);
+      if (v0 <= j0) owner0 += step;
+      if (v1 <= j1) owner1 += step;
     }
-    uint32_t const before = __shfl_sync(0xffffffffu, before_mine, owner & 31u);
-    if (j < total) {
-      StagedSegment<Amp> const& g = staging[owner];
-      uint32_t const k = j - before;
-      uint32_t bin;
-      Amp scale;
-      if (k < g.count) {
-        bin = g.start + k;
-        scale = (k == 0u && (g.flags & 1u)) ? g.first : g.mid;
-      } else {
-        bin = g.last_bin;
-        scale = g.last;
+    uint32_t const before0 = __shfl_sync(0xffffffffu, before_mine, owner0 & 31u);
+    uint32_t const before1 = __shfl_sync(0xffffffffu, before_mine, owner1 & 31u);
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      uint32_t const j = u ? j1 : j0;
+      uint32_t const owner = u ? owner1 : owner0;
+      uint32_t const before = u ? before1 : before0;
+      if (j < total) {
+        StagedSegment<Amp> const& g = staging[owner];
+        uint32_t const k = j - before;
+        uint32_t bin;
+        Amp scale;
+        if (k < g.count) {
+          bin = g.start + k;
+          scale = (k == 0u && (g.flags & 1u)) ? g.first : g.mid;
+        } else {
+          bin = g.last_bin;
+          scale = g.last;
+        }
+        deposit_bin<kFixed>(sink, bin, make_deposit<kFixed>(grid, scaled(g.perp, scale)), c.zhs,
+                            c.overflows, c.mag);
       }
-      deposit_bin<kFixed>(sink, bin, make_deposit<kFixed>(grid, scaled(g.perp, scale)), c.zhs,
-                          c.overflows, c.mag);
     }
   }
   __syncwarp();
