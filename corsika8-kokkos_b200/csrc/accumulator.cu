@@ -816,10 +816,14 @@ class Accumulator {
     uint32_t const per_chunk = ev.observer_count[0] + ev.observer_count[1];
     std::size_t chunk = tuning_.track_tile_size;
     if (chunk == 0) {
-      // about 16 work items per persistent CTA, at least 8192 tracks each
+      // about 16 work items per CTA of each launch (one CTA per SM), at least
+      // 8192 tracks each; smaller launches take chunks of an eighth of their
+      // tracks up to 262144 (fewer items, so fewer window zero/flush passes:
+      // the work list ends on quarter-size chunks anyway)
       std::size_t const ctas = static_cast<std::size_t>(sms_) * 2;
       std::size_t const target_chunks = std::max<std::size_t>(1, (16 * ctas + per_chunk - 1) / std::max<uint32_t>(per_chunk, 1));
       chunk = std::max<std::size_t>(8192, (count + target_chunks - 1) / target_chunks);
+      chunk = std::max<std::size_t>(chunk, std::min<std::size_t>((count + 7) / 8, 262144));
     }
     chunk = std::min<std::size_t>(chunk, 0x7fffffffu);
     ev.chunk_size = static_cast<uint32_t>(chunk);
