@@ -671,8 +671,8 @@ def run_e2e(pkg, showers, wl, records, precision, kernel, stream, args, torch, b
     """reset + enqueueHostLeptonTracks(pinned host records) + download(pinned traces).
 
     Host batches of 2^21 records (1.5 GB): each copy hides behind the previous
-    batch's projection, and the library starts with batches of 1/8, 1/8, 1/4
-    and 1/2 of that so the first projection waits for a short copy only."""
+    batch's projection; the library starts at an eighth of that and grows each
+    batch by a quarter, so the first projection waits for a short copy only."""
     config = showers.make_config(wl, precision=precision, kernel=kernel)
     tuning = pkg.TuningParameters(batch_size=1 << 21)
     acc = pkg.RadioAccumulator(config, tuning, stream=stream.cuda_stream)

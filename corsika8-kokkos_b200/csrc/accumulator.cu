@@ -298,12 +298,13 @@ class Accumulator {
   }
 
   // Batches of host_batch_ records (the last one partial) copied from pinned
-  // caller memory into a pair of device staging buffers (copy of batch k+1
-  // overlaps projection of batch k on the copy stream); returns after the
-  // last copy completed.  The first four batches are 1/8, 1/8, 1/4 and 1/2 of
-  // host_batch_ (together one batch), so the projection starts after a short
-  // copy and each later copy still runs behind the projection of the batch
-  // before it.
+  // caller memory into a pair of device staging buffers (the copy of batch
+  // k+1 overlaps the projection of batch k on the copy stream; a buffer is
+  // free again once its ingest has run); returns after the last copy
+  // completed.  The first batch is an eighth of host_batch_ and each next one
+  // a quarter longer, up to host_batch_: a copy takes about 0.8 of the
+  // projection of as many records, so every copy but the first stays hidden
+  // behind the projection of the batch before it, and the first is short.
   void enqueue_pinned(c8r_lepton_transport_record const* records, std::size_t count) {
     if (!copy_stream_) {
       check(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking), "copy stream");
@@ -313,12 +314,11 @@ class Accumulator {
     }
     // earlier work on the accumulator stream may still read staging_
     for (auto& e : consumed_) check(cudaEventRecord(e, stream_), "event");
-    bool const ramp = host_batch_ % 8 == 0 && host_batch_ / 8 >= 8192;
+    std::size_t size = host_batch_ / 8 >= 8192 ? host_batch_ / 8 : host_batch_;
     std::size_t offset = 0;
     for (std::size_t b = 0; offset < count; ++b) {
-      static constexpr int kRampShift[4] = {3, 3, 2, 1};
-      std::size_t const n =
-          std::min(count - offset, ramp && b < 4 ? host_batch_ >> kRampShift[b] : host_batch_);
+      std::size_t const n = std::min(count - offset, size);
+      size = std::min(host_batch_, size + size / 4);
       int const k = static_cast<int>(b & 1);
       c8r_lepton_transport_record* dst = k ? staging2_.ptr : staging_.ptr;
       // the staging buffer is free once the ingest that read it has run
@@ -328,8 +328,9 @@ class Accumulator {
             "host track upload");
       check(cudaEventRecord(copy_done_[k], copy_stream_), "event");
       check(cudaStreamWaitEvent(stream_, copy_done_[k], 0), "wait");
-      accumulate_device(dst, n, host_batch_);
+      stage_device(dst, n, host_batch_);
       check(cudaEventRecord(consumed_[k], stream_), "event");
+      project_staged(true);
       offset += n;
       stats_.host_to_device_bytes += n * sizeof(c8r_lepton_transport_record);
       ++stats_.host_track_batches;

@@ -190,8 +190,8 @@ def test_host_enqueue_batches_match_device_path(pkg, oracle, showers, torch_cuda
 def test_short_tail_items_and_ramped_pinned_batches(pkg, oracle, showers, torch_cuda):
     """Work lists that end on quarter-size chunks (the last large chunk split in
     four) and pinned host input copied straight from the caller's memory in
-    batches of 1/8, 1/8, 1/4, 1/2 and then whole host batches (the last one
-    partial) give the traces of one plain device launch."""
+    batches growing from an eighth of the host batch by a quarter each (the
+    last one partial) give the traces of one plain device launch."""
     wl, records = _workload_records(showers, "tiled_c1", 100_000, seed=41)
     want = oracle.restatement().project(showers.make_config(wl), records, threads=16)
     pinned = torch_cuda.empty(records.nbytes, dtype=torch_cuda.uint8, pin_memory=True).numpy()
@@ -213,8 +213,14 @@ def test_short_tail_items_and_ramped_pinned_batches(pkg, oracle, showers, torch_
         stats = acc.statistics()
         acc.close()
         assert_same(got, plain, True)
-        # 8192 + 8192 + 16384 + 32768, then a last partial batch of 34464
-        assert stats.host_track_batches == 5 and stats.host_tracks_enqueued == records.size
+        # batches of 8192, then each a quarter longer (up to 65536), the last one partial
+        sizes, size, left = [], 8192, records.size
+        while left:
+            sizes.append(min(size, left))
+            left -= sizes[-1]
+            size = min(65536, size + size // 4)
+        assert stats.host_track_batches == len(sizes) == 7
+        assert stats.host_tracks_enqueued == records.size
 
 
 def test_lifecycle_contracts(pkg, showers, torch_cuda):
