@@ -260,18 +260,6 @@ __device__ __forceinline__ void deposit_bin(Sink& sink, uint64_t bin, Deposit<Am
   ++contributions;
 }
 
-// One run of consecutive ZHS bins with a common value, left for the warp to
-// deposit cooperatively (count == 0: none).  Values are the fixed-point
-// integers, or the FP64 bit patterns in floating mode.
-struct PendingRange {
-  uint64_t bin;
-  uint32_t count;
-  long long v[3];
-};
-
-// Runs shorter than this are deposited by their own lane.
-constexpr uint32_t kCooperativeRun = 6;
-
 // Near-Cherenkov branch of accumulate_co_reas (RadioProjection.inl:352-387):
 // midpoint field over the Doppler-compressed duration.  Kept out of line: it
 // is taken by a minority of pairs, and its third propagation would otherwise
@@ -467,15 +455,11 @@ __device__ __noinline__ Counts zhs_indexed_bins(ObserverCache const& o, Sink sin
 // The multi-bin tail of a ZHS segment (first sample and intermediate bins,
 // RadioProjection.inl:457-472), out of line: about half the segments take it,
 // and keeping it out of the common path saves registers and instruction fetch.
-// A run of intermediate bins left for the warp is returned in `run` when
-// want_run.
 template <bool kFixed, bool kRuns, class Amp, class Sink>
 __device__ __noinline__ Counts zhs_multi_tail(ObserverCache const& o, Sink sink, double d1,
                                               double x1, double sb, int nb, Vec3<Amp> perp,
-                                              double sc, double dd, double mc, bool run_ok,
-                                              bool want_run, PendingRange& run) {
+                                              double sc, double dd, double mc, bool run_ok) {
   Counts c;
-  PendingRange* pending = want_run ? &run : nullptr;
   double const frac_first = fabs(sb + 0.5 - x1);
   add_sample<true, kFixed>(o, sink, d1,
                            scaled(perp, amp_div(static_cast<Amp>(sc * frac_first), static_cast<Amp>(dd))),
@@ -492,23 +476,8 @@ __device__ __noinline__ Counts zhs_multi_tail(ObserverCache const& o, Sink sink,
       if (hi > lo) {
         uint64_t const first = static_cast<uint64_t>(b1 + lo);
         uint32_t const count = static_cast<uint32_t>(hi - lo);
-        bool const all_ok = !kFixed || (mid.okx && mid.oky && mid.okz);
-        if (pending && all_ok && count >= kCooperativeRun && pending->count == 0) {
-          pending->bin = first;
-          pending->count = count;
-          if (kFixed) {
-            pending->v[0] = mid.ix;
-            pending->v[1] = mid.iy;
-            pending->v[2] = mid.iz;
-          } else {
-            pending->v[0] = __double_as_longlong(static_cast<double>(mid.value.x));
-            pending->v[1] = __double_as_longlong(static_cast<double>(mid.value.y));
-            pending->v[2] = __double_as_longlong(static_cast<double>(mid.value.z));
-          }
-        } else {
-          for (uint32_t j = 0; j < count; ++j)
-            deposit_bin<kFixed>(sink, first + j, mid, c.zhs, c.overflows, c.mag);
-        }
+        for (uint32_t j = 0; j < count; ++j)
+          deposit_bin<kFixed>(sink, first + j, mid, c.zhs, c.overflows, c.mag);
       }
     } else {
       Counts const d = zhs_indexed_bins<kFixed, Amp>(o, sink, d1, x1, nb, mid);
@@ -525,9 +494,9 @@ __device__ __noinline__ Counts zhs_multi_tail(ObserverCache const& o, Sink sink,
 // kRuns = true (windowed kernel): the intermediate bins of a segment are the
 // consecutive bins nearest(x1) + i whenever x1 lies farther than a rounding
 // bound from a half bin (checked below); they are then deposited as one run,
-// without the per-index division, and long runs are handed to the warp via
-// `pending`.  Otherwise, and always for kRuns = false (the reference-shaped
-// direct kernel), each index is binned by the reference's own expression.
+// without the per-index division.  Otherwise, and always for kRuns = false
+// (the reference-shaped direct kernel), each index is binned by the
+// reference's own expression.
 //
 // kFilter = true (mixed precision): the emission direction is d * RN(1/|d|),
 // so n beta.k lies within e_nbk of the reference's value and each detection
@@ -541,7 +510,7 @@ __device__ __forceinline__ bool zhs_segment(double p1x, double p1y, double p1z, 
                                             double p2y, double p2z, double t1, double t2,
                                             Track const& t, Propagation const& p,
                                             ObserverCache const& o, Sink& sink, Counts& c,
-                                            bool subdivided, PendingRange* pending) {
+                                            bool subdivided) {
   double const mx = (p1x + p2x) * 0.5, my = (p1y + p2y) * 0.5, mz = (p1z + p2z) * 0.5;
   Path const path = propagate<true, kFilter>(p, o, mx, my, mz);
   double const bk = t.bx * path.kx + t.by * path.ky + t.bz * path.kz;
@@ -610,15 +579,11 @@ __device__ __forceinline__ bool zhs_segment(double p1x, double p1y, double p1z, 
                                                 static_cast<Amp>(den_last))),
                            c.zhs, c.overflows, c.mag);
   if (single) return true;
-  PendingRange run;
-  run.count = 0;
   Counts const d = zhs_multi_tail<kFixed, kRuns, Amp>(
-      o, sink, d1, x1, sb, nb, perp, sc, dd, (subdivided ? 1. : sign) * t.constant, run_ok,
-      pending != nullptr && pending->count == 0, run);
+      o, sink, d1, x1, sb, nb, perp, sc, dd, (subdivided ? 1. : sign) * t.constant, run_ok);
   c.zhs += d.zhs;
   c.overflows += d.overflows;
   c.mag += d.mag;
-  if (run.count) *pending = run;
   return true;
 }
 
@@ -814,8 +779,7 @@ __device__ __forceinline__ void deposit_staged(StagedSegment<Amp>* staging,
 // accumulate_zhs, RadioProjection.inl:483-529, every decision exact.
 template <bool kFixed, bool kRuns, class Amp, class Sink>
 __device__ __forceinline__ void zhs_pair(Track const& t, Propagation const& p,
-                                         ObserverCache const& o, Sink& sink, Counts& c,
-                                         PendingRange* pending) {
+                                         ObserverCache const& o, Sink& sink, Counts& c) {
   double const mx = (t.sx + t.ex) * 0.5, my = (t.sy + t.ey) * 0.5, mz = (t.sz + t.ez) * 0.5;
   Path const pm = propagate<false>(p, o, mx, my, mz);
   double const uk = (t.bx * pm.kx + t.by * pm.ky + t.bz * pm.kz) / t.beta_module;
@@ -852,7 +816,7 @@ __device__ __forceinline__ void zhs_pair(Track const& t, Propagation const& p,
   for (long long index = 0; index < segments; ++index) {
     double const p2x = p1x + rx, p2y = p1y + ry, p2z = p1z + rz, t2 = t1 + rt;
     zhs_segment<kFixed, kRuns, false, Amp>(p1x, p1y, p1z, p2x, p2y, p2z, t1, t2, t, p, o, sink, c,
-                                           subdivided, pending);
+                                           subdivided);
     p1x = p2x;
     p1y = p2y;
     p1z = p2z;
@@ -1181,7 +1145,7 @@ __global__ void __launch_bounds__(256) direct_kernel(const __grid_constant__ Eve
         sink.row[r] = kFixed ? ev.fixed[1] + r * ev.total_bins[1] + o.offset : nullptr;
         sink.frow[r] = kFixed ? nullptr : ev.floating[1] + r * ev.total_bins[1] + o.offset;
       }
-      zhs_pair<kFixed, false, Amp>(t, ev.propagation, o, sink, c, nullptr);
+      zhs_pair<kFixed, false, Amp>(t, ev.propagation, o, sink, c);
     }
   }
   flush_counts(c, ev.counters);
@@ -1297,7 +1261,7 @@ __device__ __noinline__ Counts zhs_drain(const double* __restrict__ tracks, uint
         seg.count = 0u;
         seg.flags = 0u;
         zhs_segment<kFixed, true, false, Amp>(p1x, p1y, p1z, p2x, p2y, p2z, t1, t2, t, p, o, sink,
-                                              c, subdivided, nullptr);
+                                              c, subdivided);
       }
       p1x = p2x;
       p1y = p2y;
