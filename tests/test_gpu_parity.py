@@ -223,6 +223,24 @@ def test_short_tail_items_and_ramped_pinned_batches(pkg, oracle, showers, torch_
         assert stats.host_tracks_enqueued == records.size
 
 
+def test_growing_host_batches_grow_the_deferred_lists(pkg, oracle, showers, torch_cuda):
+    """Pinned host batches that grow (automatic chunks from 8192 to 10000 tracks)
+    make the accumulator grow its per-CTA deferred-pair lists between launches;
+    the traces equal the oracle's."""
+    wl, records = _workload_records(showers, "plain_c0", 300_000, seed=43)
+    pinned = torch_cuda.empty(records.nbytes, dtype=torch_cuda.uint8, pin_memory=True).numpy()
+    pinned[:] = records.view(np.uint8)
+    config = showers.make_config(wl, kernel=KERNELS["windowed"])
+    acc = pkg.RadioAccumulator(config, pkg.TuningParameters(batch_size=262144))
+    acc.enqueue_host_lepton_tracks(pinned.view(pkg.LEPTON_RECORD))
+    got = acc.download_fixed()
+    stats = acc.statistics()
+    acc.close()
+    want = oracle.restatement().project(config, records, threads=16)
+    assert_same(got, want, True)
+    assert stats.host_track_batches == 6 and stats.host_tracks_enqueued == records.size
+
+
 def test_lifecycle_contracts(pkg, showers, torch_cuda):
     """Rejection contracts of testRadioAccumulator.cpp:216-302."""
     wl, records = _workload_records(showers, "plain_c0", 100, seed=1)
