@@ -301,11 +301,25 @@ def run_ours(args):
     zhs_ms = stats.zhs_kernel_time_ms / args.steps
     coreas_ms = stats.coreas_kernel_time_ms / args.steps
     peak = peaks["fp64_flops"] / 1e12
-    traffic = {}
+    traffic, instructions = {}, {}
     traffic_file = ROOT / "profiles" / "windowed_traffic.json"
     if traffic_file.exists():
         t = json.loads(traffic_file.read_text())
         traffic = {"zhs": t["zhs_bytes_per_track"] * n, "coreas": t["coreas_bytes_per_track"] * n}
+        instructions = {k: t.get(f"{k}_warp_instructions_per_pair") for k in ("zhs", "coreas")}
+    # issue roofline: 4 warp instructions per clock per SM (one per scheduler)
+    sms = torch.cuda.get_device_properties(local).multi_processor_count
+    issue_peak = 4 * sms * (clocks.get("sm_mhz") or 0) * 1e6
+
+    def issue(key, ms):
+        per_pair = instructions.get(key)
+        if not per_pair or not ms or not issue_peak:
+            return None
+        achieved = per_pair * pairs_per_step / (ms * 1e-3)
+        return {"warp_instructions_per_pair": per_pair, "achieved_per_s": achieved,
+                "peak_per_s": issue_peak, "frac": achieved / issue_peak,
+                "source": "instructions per pair from the ncu capture in profiles/; peak = 4 x SMs "
+                          "x the SM clock sampled during the timed steps"}
 
     def roof(flops, ms, key):
         achieved = flops / (ms * 1e-3) / 1e12 if ms > 0 else None
@@ -324,8 +338,9 @@ def run_ours(args):
         "hbm": {"bytes_per_launch": traffic.get("zhs"),
                 "achieved_gbs": (traffic.get("zhs") or 0) / (zhs_ms * 1e-3) / 1e9 if zhs_ms else None,
                 "peak_gbs": hbm_peak_gbs()},
+        "issue": issue("zhs", zhs_ms),
         "secondary": dict(roof(coreas_flops, coreas_ms, "coreas"),
-                          kernel="windowed_kernel<fixed,float,CoREAS>"),
+                          kernel="windowed_kernel<fixed,float,CoREAS>", issue=issue("coreas", coreas_ms)),
         "atomics": {"shared_per_s_peak": peaks["shared_atomics_per_s"],
                     "global_per_s_peak": peaks["global_atomics_per_s"],
                     "samples_per_s": (per["coreas_contributions"] + per["zhs_contributions"]) /
