@@ -352,6 +352,14 @@ def run_ours(args):
         e2e = run_e2e(pkg, showers, wl, records, precision, kernel, stream, args, torch, barrier,
                       max_over_ranks, world)
 
+    # the served stream runs before the CPU baseline: its latencies depend on the
+    # host threads that feed it, which the baseline's worker threads would crowd
+    serving = None
+    if rank == 0 and world == 1 and not args.no_serving:
+        del device_records
+        torch.cuda.empty_cache()
+        serving = run_serving(pkg, showers, torch, args, local)
+
     baseline = None
     if rank == 0 and world == 1 and not args.no_baseline:
         sample = records[: args.baseline_segments]
@@ -360,12 +368,6 @@ def run_ours(args):
         baseline = {"value": bpairs / btimes[0], "unit": "pairs/s", "cores": threads, "kind": kind,
                     "sample": f"first {sample.size} of {n} segments x {observers} antennas "
                               f"({bpairs:.3g} pairs), fixed-point CoREAS+ZHS, one pass"}
-
-    serving = None
-    if rank == 0 and world == 1 and not args.no_serving:
-        del device_records
-        torch.cuda.empty_cache()
-        serving = run_serving(pkg, showers, torch, args, local)
 
     if world > 1:
         dist.destroy_process_group()

@@ -346,15 +346,6 @@ __device__ __forceinline__ void coreas_pair(Track const& t, Propagation const& p
   add_sample<false, kFixed>(o, sink, er, fend, c.coreas, c.overflows, c.mag);
 }
 
-// The exact pair out of line: the filtered path's fallback.
-template <bool kFixed, class Amp, class Sink>
-__device__ __noinline__ Counts coreas_pair_exact(Track const t, Propagation const& p,
-                                                 ObserverCache const& o, Sink sink) {
-  Counts c;
-  coreas_pair<kFixed, Amp>(t, p, o, sink, c);
-  return c;
-}
-
 // The propagation of the filtered paths: propagate_fast when kFast, else the
 // exact propagate (time_err 0).
 template <bool kFast>
@@ -368,7 +359,7 @@ __device__ __forceinline__ FastPath filtered_path(Propagation const& p, Observer
 // The common CoREAS pair of the windowed kernel (RadioProjection.inl:339-409
 // without its near-Cherenkov branch).  Returns false, having deposited
 // nothing, when the pair needs the near-Cherenkov branch or (kFilter) an exact
-// evaluation; the kernel then defers it to coreas_pair_exact.
+// evaluation; the kernel then defers it to coreas_drain_pair.
 //
 // kFilter (mixed precision): travel times, refractive indices and distances
 // are exact; emission directions are d * RN(1/|d|) (propagate's
@@ -1284,6 +1275,17 @@ __device__ __noinline__ Counts zhs_drain(const double* __restrict__ tracks, uint
   return c;
 }
 
+// A deferred CoREAS pair of the windowed kernel, loaded and evaluated exactly
+// out of line (the caller passes the row, not the 112-byte track).
+template <bool kFixed, class Amp, class Sink>
+__device__ __noinline__ Counts coreas_drain_pair(const double* __restrict__ tracks, uint64_t row,
+                                                 Propagation const& p, ObserverCache const& o,
+                                                 Sink sink) {
+  Counts c;
+  coreas_pair<kFixed, Amp>(load_track(tracks, 0, row), p, o, sink, c);
+  return c;
+}
+
 template <bool kFixed, class Amp, int kAlgorithm>
 __global__ void __launch_bounds__(kAlgorithm == 1 ? kZhsThreadsMax : kWindowThreadsMax, 1)
     windowed_kernel(const __grid_constant__ WorkPlan plan) {
@@ -1392,8 +1394,8 @@ __global__ void __launch_bounds__(kAlgorithm == 1 ? kZhsThreadsMax : kWindowThre
           d = zhs_drain<kFixed, kFilter, Amp>(ev.tracks, begin, deferred_list + from, count,
                                               ev.propagation, o, sink, staging);
         } else if (lane < count) {
-          Track const t = load_track(ev.tracks, ev.stride, begin + deferred_list[from + lane]);
-          d = coreas_pair_exact<kFixed, Amp>(t, ev.propagation, o, sink);
+          d = coreas_drain_pair<kFixed, Amp>(ev.tracks, begin + deferred_list[from + lane],
+                                             ev.propagation, o, sink);
         }
         c.coreas += d.coreas;
         c.zhs += d.zhs;
