@@ -73,14 +73,14 @@ struct WorkPlan {
   uint32_t window;          // shared-memory bins per CTA (max over events)
   uint64_t total_items;
   unsigned int* next_item;  // zeroed before each launch
-  // ZHS launches: each CTA's list of the deferred pairs of its current item,
+  // Each CTA's list of the deferred pairs of its current item,
   // `deferred_stride` entries from deferred + blockIdx.x * deferred_stride
   // (at least the longest chunk of the plan; deferred_list_stride below).
   unsigned int* deferred;
   uint32_t deferred_stride;
 };
 
-// Entries per CTA of a ZHS launch's deferred lists: the plan's longest chunk.
+// Entries per CTA of a launch's deferred lists: the plan's longest chunk.
 inline uint32_t deferred_list_stride(WorkPlan const& plan) {
   uint32_t stride = 0;
   for (uint32_t e = 0; e < plan.event_count; ++e)
@@ -151,8 +151,8 @@ cudaError_t launch_direct(EventPlan const& event, uint64_t track_bound, bool cor
                           bool fixed, Precision precision, cudaStream_t stream);
 
 // Persistent windowed kernel.  `ctas` persistent CTAs of `threads` threads.
-// A ZHS plan (algorithm 1) needs plan.deferred with ctas * deferred_stride
-// entries and deferred_stride >= deferred_list_stride(plan).
+// The plan needs plan.deferred with ctas * deferred_stride entries and
+// deferred_stride >= deferred_list_stride(plan) (else cudaErrorInvalidValue).
 cudaError_t launch_windowed(WorkPlan const& plan, bool fixed, Precision precision, int ctas,
                             int threads, cudaStream_t stream);
 // Largest window (bins) that fits the opt-in shared memory of this device.
