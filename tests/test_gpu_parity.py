@@ -241,6 +241,25 @@ def test_growing_host_batches_grow_the_deferred_lists(pkg, oracle, showers, torc
     assert stats.host_track_batches == 6 and stats.host_tracks_enqueued == records.size
 
 
+def test_side_stream_and_serial_launches_agree(pkg, showers, torch_cuda):
+    """Without kernel timing the ZHS launch runs on a second stream beside the
+    CoREAS launch; with it both run on the accumulator's stream.  Fixed-point
+    traces and counters are the same either way, in both precisions."""
+    wl, records = _workload_records(showers, "tiled_c1", 30_000, seed=47)
+    raw = to_device(torch_cuda, records)
+    for precision in (0, 1):
+        config = showers.make_config(wl, precision=precision, kernel=KERNELS["windowed"])
+        results = []
+        for timing in (False, True):
+            acc = pkg.RadioAccumulator(config)
+            acc.set_kernel_timing(timing)
+            for _ in range(2):  # two accumulates: the second waits for the first's ZHS launch
+                acc.accumulate_lepton_tracks(raw.data_ptr(), records.size)
+            results.append(acc.download_fixed())
+            acc.close()
+        assert_same(results[0], results[1], True)
+
+
 def test_lifecycle_contracts(pkg, showers, torch_cuda):
     """Rejection contracts of testRadioAccumulator.cpp:216-302."""
     wl, records = _workload_records(showers, "plain_c0", 100, seed=1)
