@@ -75,6 +75,7 @@ PRECISION_STUDY_FP64 = 4
 KERNEL_AUTO = 0
 KERNEL_DIRECT = 1
 KERNEL_WINDOWED = 2
+KERNEL_TILED = 3
 BATCH_GRAPH = 1
 BATCH_KEEP_STAGED = 2
 
@@ -204,6 +205,7 @@ class Statistics(C.Structure):
         ("coreas_kernel_time_ms", C.c_double),
         ("zhs_kernel_time_ms", C.c_double),
         ("counters", Counters),
+        ("window_reruns", C.c_uint64),
     ]
 
 
@@ -226,6 +228,25 @@ class TrackColumns(C.Structure):
                 ("end_time_s", C.c_void_p), ("start_energy_gev", C.c_void_p),
                 ("start_position_m", C.c_void_p * 3), ("end_position_m", C.c_void_p * 3),
                 ("start_direction", C.c_void_p * 3), ("end_direction", C.c_void_p * 3)]
+
+
+class FixedSnapshot(C.Structure):
+    """c8r_fixed_snapshot: a view of one endpoint's FixedRadioSnapshot."""
+    _fields_ = [
+        ("shower_identity", C.c_char_p),
+        ("endpoint", C.c_uint32),
+        ("reserved_", C.c_uint32),
+        ("config", C.POINTER(Config)),
+        ("coreas", C.c_void_p),
+        ("coreas_count", C.c_size_t),
+        ("zhs", C.c_void_p),
+        ("zhs_count", C.c_size_t),
+        ("counters", Counters),
+    ]
+
+
+ENDPOINT_CUDA = 0
+ENDPOINT_OPENMP = 1
 
 
 class ServerOptions(C.Structure):
@@ -315,6 +336,18 @@ PROTOTYPES = {
     "c8r_accumulate_columns": (C.c_int, [C.c_void_p, C.POINTER(TrackColumns), C.c_size_t]),
     "c8r_download_fields_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(Counters)]),
     "c8r_merge_fixed": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t]),
+    "c8r_download_fixed_snapshot": (C.c_int, [C.c_void_p, C.c_char_p, C.c_uint32, C.c_void_p, C.c_void_p,
+                                              C.POINTER(Counters)]),
+    "c8r_snapshot_bins": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
+    "c8r_validate_fixed_snapshot": (C.c_int, [C.POINTER(FixedSnapshot)]),
+    "c8r_merge_counters": (C.c_int, [C.POINTER(Counters), C.POINTER(Counters)]),
+    "c8r_snapshot_last_error": (C.c_char_p, []),
+    "c8r_cooperative_merge_create": (C.c_int, [C.c_char_p, C.POINTER(Config), C.POINTER(C.c_void_p)]),
+    "c8r_cooperative_merge_destroy": (None, [C.c_void_p]),
+    "c8r_cooperative_merge_last_error": (C.c_char_p, [C.c_void_p]),
+    "c8r_cooperative_merge_commit": (C.c_int, [C.c_void_p, C.POINTER(FixedSnapshot)]),
+    "c8r_cooperative_merge_take": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(Counters),
+                                             C.POINTER(C.c_uint32)]),
     "c8r_spool_writer_create": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
     "c8r_spool_append": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t]),
     "c8r_spool_complete": (C.c_int, [C.c_void_p]),

@@ -22,16 +22,13 @@
 #include "../../include/c8radio.h"
 #include "host_setup.hpp"
 #include "radio_kernels.cuh"
+#include "status.hpp"
 
 namespace c8r {
 namespace {
 
 constexpr std::size_t kDefaultHostBatch = 4096;   // RadioAccumulator.hpp:49
 constexpr std::size_t kDirectThreshold = 16384;   // RadioAccumulator.hpp:101
-
-struct cuda_error : std::runtime_error {
-  using std::runtime_error::runtime_error;
-};
 
 void check(cudaError_t err, char const* what) {
   if (err != cudaSuccess)
@@ -125,7 +122,7 @@ void validate(c8r_config const& config) {
     throw std::invalid_argument("invalid flat-atmosphere radio snapshot");
   if (config.precision < C8R_PRECISION_FP64 || config.precision > C8R_PRECISION_STUDY_FP64)
     throw std::invalid_argument("invalid radio precision");
-  if (config.kernel < C8R_KERNEL_AUTO || config.kernel > C8R_KERNEL_WINDOWED)
+  if (config.kernel < C8R_KERNEL_AUTO || config.kernel > C8R_KERNEL_TILED)
     throw std::invalid_argument("invalid radio kernel selection");
   if (config.count_samples && !config.deterministic)
     throw std::invalid_argument("radio sample counting needs fixed-point traces");
@@ -195,6 +192,12 @@ class Accumulator {
     tuning_ = tuning;
     if (!enabled_) return;
     validate(config);
+    // snapshot extents: every configured observer, its algorithm enabled or not
+    config_bins_[0] = total_bins(config.coreas_observers, config.coreas_observer_count);
+    config_bins_[1] = total_bins(config.zhs_observers, config.zhs_observer_count);
+    for (std::size_t bins : config_bins_)
+      if (bins > std::numeric_limits<std::size_t>::max() / 3)
+        throw std::overflow_error("radio waveform bin overflow");
     check(cudaGetDevice(&device_), "cudaGetDevice");
     check(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, device_), "SM count");
     copy_config(config);
@@ -207,10 +210,12 @@ class Accumulator {
     host_batch_ = tuning.batch_size ? static_cast<std::size_t>(tuning.batch_size) : kDefaultHostBatch;
     threads_ = tuning.team_size ? static_cast<int>(tuning.team_size) : kWindowThreads;
     upload_static();
+    choose_ingest_terms();
     allocate_traces();
     counters_.allocate(1);
     slot_.allocate(1);
     next_item_.allocate(2);  // one work counter per algorithm
+    reruns_.allocate(1);
     staging_.allocate(host_batch_);
     for (auto& h : host_) h.allocate(host_batch_);
     for (auto& e : host_ready_) check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
@@ -253,6 +258,7 @@ class Accumulator {
         check(cudaMemsetAsync(float_traces_[a].ptr, 0, float_traces_[a].bytes(), stream_), "memset");
     }
     check(cudaMemsetAsync(counters_.ptr, 0, sizeof(DeviceCounters), stream_), "memset");
+    check(cudaMemsetAsync(reruns_.ptr, 0, sizeof(unsigned long long), stream_), "memset");
     clear_staged();
     check(cudaStreamSynchronize(stream_), "reset fence");
     resolve_timing();
@@ -378,7 +384,7 @@ class Accumulator {
     ensure_capacity(staged_ + count);
     if (staged_ == 0) check(cudaMemsetAsync(slot_.ptr, 0, sizeof(unsigned long long), stream_), "memset");
     check(launch_ingest(records, count, tracks_.ptr, capacity_, slot_.ptr, counters_.ptr,
-                        diagnostics_, stream_),
+                        diagnostics_, terms_, stream_),
           "ingest launch");
     staged_ += count;
     ++stats_.track_precompute_batches;
@@ -403,7 +409,7 @@ class Accumulator {
     ensure_capacity(staged_ + count);
     if (staged_ == 0) check(cudaMemsetAsync(slot_.ptr, 0, sizeof(unsigned long long), stream_), "memset");
     check(launch_ingest_columns(columns, count, tracks_.ptr, capacity_, slot_.ptr, counters_.ptr, diagnostics_,
-                                stream_),
+                                terms_, stream_),
           "ingest launch");
     staged_ += count;
     ++stats_.track_precompute_batches;
@@ -427,6 +433,8 @@ class Accumulator {
                         (kernel_ == C8R_KERNEL_AUTO && count < kDirectThreshold);
     if (study_)
       project_study(count);
+    else if (kernel_ == C8R_KERNEL_TILED)
+      project_tiled(count);
     else if (direct)
       project_direct(count);
     else
@@ -594,13 +602,56 @@ class Accumulator {
     downloaded_ = true;
   }
 
+  // RadioAccumulator::downloadFixed(shower_identity, endpoint), RadioAccumulator.inl:359-405:
+  // the reference's checks in its order.  After the pending host batch is
+  // flushed the identity and endpoint are checked (nothing sealed yet); then
+  // the endpoint is sealed before the copies, so a failed export cannot be
+  // repeated or followed by download(), and the snapshot is validated after
+  // them (validate_fixed_radio: an overflowed accumulator is rejected, still
+  // sealed).  Each buffer holds 3 x the bins of every configured observer of
+  // its algorithm; a disabled algorithm's traces are zero, as the reference's.
+  void download_fixed_snapshot(char const* identity, unsigned endpoint, long long* coreas, long long* zhs,
+                               c8r_counters* counters) {
+    if (!enabled() || !fixed_ || downloaded_ || sealed_)
+      throw std::logic_error("fixed radio snapshot unavailable/already committed");
+    flush();
+    project_staged(true);
+    if (identity == nullptr || identity[0] == '\0' || endpoint > 1)
+      throw std::invalid_argument("invalid cooperative radio snapshot identity");
+    if ((config_bins_[0] && coreas == nullptr) || (config_bins_[1] && zhs == nullptr))
+      throw std::invalid_argument("null radio snapshot trace buffer");
+    sealed_ = true;
+    DeviceCounters host{};
+    fetch_counters(host);
+    for (int a = 0; a < 2; ++a) {
+      long long* out = a == 0 ? coreas : zhs;
+      std::size_t const values = 3 * config_bins_[a];
+      if (values == 0) continue;
+      if (fixed_traces_[a].ptr && bins_[a] == config_bins_[a]) {
+        check(cudaMemcpyAsync(out, fixed_traces_[a].ptr, values * sizeof(long long),
+                              cudaMemcpyDeviceToHost, stream_),
+              "fixed trace download");
+        stats_.device_to_host_bytes += values * sizeof(long long);
+      } else {
+        std::memset(out, 0, values * sizeof(long long));  // algorithm disabled
+      }
+    }
+    check(cudaStreamSynchronize(stream_), "download fence");
+    if (counters) std::memcpy(counters, &host, sizeof(host));
+    if (host.fixed_point_overflows != 0)
+      throw std::invalid_argument("invalid/overflowed cooperative fixed radio snapshot");
+    downloaded_ = true;
+  }
+
+  std::size_t config_bins(int a) const { return config_bins_[a]; }
+
   void statistics(c8r_statistics& out) {
     resolve_timing();
     out = stats_;
   }
 
   std::size_t device_bytes() const {
-    std::size_t total = table_.bytes() + counters_.bytes() + slot_.bytes() + next_item_.bytes() +
+    std::size_t total = table_.bytes() + counters_.bytes() + slot_.bytes() + next_item_.bytes() + reruns_.bytes() +
                         staging_.bytes() + staging2_.bytes() + tracks_.bytes() + deferred_[0].bytes() +
                         deferred_[1].bytes();
     for (int a = 0; a < 2; ++a)
@@ -763,6 +814,20 @@ class Accumulator {
     if (window_bins_ == 0) window_bins_ = 1;
   }
 
+  // Source terms precomputed at ingest when every observer of both enabled
+  // algorithms shares one destination row (always in a homogeneous medium).
+  void choose_ingest_terms() {
+    std::vector<ObserverCache> all;
+    for (int a = 0; a < 2; ++a)
+      if (a == 0 ? coreas_enabled_ : zhs_enabled_)
+        all.insert(all.end(), observers_host_[a].begin(), observers_host_[a].end());
+    Destination d{};
+    terms_ = IngestTerms{};
+    terms_.enabled = shared_destination(all.data(), all.size(), d) ? 1 : 0;
+    terms_.propagation = propagation_;
+    terms_.destination = d;
+  }
+
   void allocate_traces() {
     for (int a = 0; a < 2; ++a) {
       std::size_t const values = 3 * bins_[a];
@@ -831,6 +896,7 @@ class Accumulator {
     ev.chunks = static_cast<uint32_t>((count + chunk - 1) / chunk);
     ev.first_track = 0;
     ev.last_track = ~0ull;
+    ev.precomputed = static_cast<uint32_t>(terms_.enabled);
     return ev;
   }
 
@@ -863,6 +929,24 @@ class Accumulator {
     if (fuse_) stats_.fused_track_observer_pairs += pairs_c;
     ++stats_.direct_projection_batches;
     stats_.direct_projection_records += count;
+  }
+
+  // The reference's tile shape (RadioAccumulator.inl:699-847): fused when the
+  // observer grids match, else one launch per algorithm.
+  void project_tiled(std::size_t count) {
+    EventPlan const ev = make_event(count);
+    bool const c = ev.observer_count[0] != 0, z = ev.observer_count[1] != 0;
+    if (fuse_) {
+      check(launch_tiled(ev, count, true, true, fixed_, precision_, stream_), "tiled launch");
+    } else {
+      if (c) check(launch_tiled(ev, count, true, false, fixed_, precision_, stream_), "tiled launch");
+      if (z) check(launch_tiled(ev, count, false, true, fixed_, precision_, stream_), "tiled launch");
+    }
+    uint64_t const pairs_c = count * ev.observer_count[0], pairs_z = count * ev.observer_count[1];
+    stats_.track_observer_pairs += pairs_c + pairs_z;
+    if (fuse_) stats_.fused_track_observer_pairs += pairs_c;
+    uint64_t const observers = std::max(ev.observer_count[0], ev.observer_count[1]);
+    stats_.projection_tiles += ((count + 7) / 8) * ((observers + 31) / 32);
   }
 
   // The precision study's generic kernel, both algorithms in one launch.
@@ -902,6 +986,7 @@ class Accumulator {
       plan.algorithm = algorithm;
       plan.window = ev.window;
       plan.next_item = next_item_.ptr + algorithm;
+      plan.reruns = reruns_.ptr;
       uint64_t ctas = static_cast<uint64_t>(per_sm) * sms_;
       append_work(plan, ev, ctas, true);
       if (ctas > plan.total_items) ctas = plan.total_items;
@@ -935,6 +1020,9 @@ class Accumulator {
   void fetch_counters(DeviceCounters& host) {
     check(cudaMemcpyAsync(&host, counters_.ptr, sizeof(host), cudaMemcpyDeviceToHost, stream_),
           "counter download");
+    check(cudaMemcpyAsync(&stats_.window_reruns, reruns_.ptr, sizeof(unsigned long long),
+                          cudaMemcpyDeviceToHost, stream_),
+          "counter download");
     check(cudaStreamSynchronize(stream_), "counter fence");
     stats_.lepton_tracks = host.valid_tracks;
     stats_.coreas_contributions = host.coreas_contributions;
@@ -961,10 +1049,12 @@ class Accumulator {
   double limit_ = 1.;
   c8r_tuning tuning_{};
   Propagation propagation_{};
+  IngestTerms terms_{};  // source terms written at ingest (enabled: shared destination row)
   std::vector<double2> table_host_;
   std::vector<c8r_observer_snapshot> snapshots_[2];
   std::vector<ObserverCache> observers_host_[2];
   std::size_t bins_[2] = {0, 0};
+  std::size_t config_bins_[2] = {0, 0};  // all configured observers (snapshot extents)
   uint64_t max_observer_bins_[2] = {0, 0};
   std::size_t window_bins_ = 0;
   DeviceBuffer<double2> table_;
@@ -977,6 +1067,7 @@ class Accumulator {
   DeviceBuffer<DeviceCounters> counters_;
   DeviceBuffer<unsigned long long> slot_;
   DeviceBuffer<unsigned> next_item_;
+  DeviceBuffer<unsigned long long> reruns_;  // windowed items re-run with checked adds
   DeviceBuffer<unsigned> deferred_[2];  // per-CTA deferred-pair lists, by algorithm
   DeviceBuffer<double> tracks_;
   std::size_t capacity_ = 0;
@@ -1226,40 +1317,7 @@ namespace {
 
 thread_local std::string g_last_error;
 
-template <class F>
-int guarded(std::string* error, F&& body) {
-  try {
-    body();
-    return C8R_OK;
-  } catch (std::invalid_argument const& e) {
-    if (error) *error = e.what();
-    return C8R_INVALID_ARGUMENT;
-  } catch (std::out_of_range const& e) {
-    if (error) *error = e.what();
-    return C8R_OUT_OF_RANGE;
-  } catch (std::length_error const& e) {
-    if (error) *error = e.what();
-    return C8R_LENGTH_ERROR;
-  } catch (std::logic_error const& e) {
-    if (error) *error = e.what();
-    return C8R_LOGIC_ERROR;
-  } catch (std::overflow_error const& e) {
-    if (error) *error = e.what();
-    return C8R_OVERFLOW_ERROR;
-  } catch (c8r::cuda_error const& e) {
-    if (error) *error = e.what();
-    return C8R_CUDA_ERROR;
-  } catch (std::runtime_error const& e) {
-    if (error) *error = e.what();
-    return C8R_RUNTIME_ERROR;
-  } catch (std::bad_alloc const&) {
-    if (error) *error = "radio allocation failed";
-    return C8R_BAD_ALLOC;
-  } catch (...) {
-    if (error) *error = "unknown radio failure";
-    return C8R_RUNTIME_ERROR;
-  }
-}
+using c8r::guarded;
 
 int with_handle(c8r_accumulator const* h, std::string* error_slot, bool need) {
   (void)error_slot;
@@ -1366,6 +1424,21 @@ int c8r_download_fixed(c8r_accumulator* handle, long long* coreas_xyz, long long
   if (int s = with_handle(handle, nullptr, true)) return s;
   return guarded(&handle->error,
                  [&] { handle->impl->download_fixed(coreas_xyz, zhs_xyz, counters); });
+}
+
+int c8r_download_fixed_snapshot(c8r_accumulator* handle, const char* shower_identity, uint32_t endpoint,
+                                long long* coreas_xyz, long long* zhs_xyz, c8r_counters* counters) {
+  if (int s = with_handle(handle, nullptr, true)) return s;
+  return guarded(&handle->error, [&] {
+    handle->impl->download_fixed_snapshot(shower_identity, endpoint, coreas_xyz, zhs_xyz, counters);
+  });
+}
+
+int c8r_snapshot_bins(const c8r_accumulator* handle, size_t* coreas_bins, size_t* zhs_bins) {
+  if (int s = with_handle(handle, nullptr, true)) return s;
+  if (coreas_bins) *coreas_bins = handle->impl->config_bins(0);
+  if (zhs_bins) *zhs_bins = handle->impl->config_bins(1);
+  return C8R_OK;
 }
 
 int c8r_accumulate_columns(c8r_accumulator* handle, const c8r_track_columns* columns, size_t count) {

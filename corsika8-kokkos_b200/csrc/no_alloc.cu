@@ -108,35 +108,94 @@ DeviceSetup const& setup_current_device() {
   return s;
 }
 
-// The accumulator's per-observer constants (make_observer_cache), built 32
-// at a time on the host stack and copied into scratch.
+// Host data reaches the scratch array as the by-value parameter of a copy
+// kernel: the launch copies its parameters when it is queued, so the call
+// neither waits for earlier work on `stream` nor depends on the kind of host
+// memory the caller's arrays are in (a cudaMemcpyAsync from pageable memory
+// would synchronise, and one from pinned memory would read it later).
+constexpr std::size_t kUploadBytes = 16384;
+struct UploadBlock {
+  uint4 words[kUploadBytes / sizeof(uint4)];
+};
+
+__global__ void upload_kernel(const __grid_constant__ UploadBlock block, uint4* __restrict__ out,
+                              uint32_t words) {
+  for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) out[i] = block.words[i];
+}
+
+// Queues a copy of `bytes` (a multiple of 16, at most kUploadBytes) from the
+// host block to device address `out` (16-byte aligned).
+void upload(UploadBlock const& block, void* out, std::size_t bytes, cudaStream_t stream) {
+  uint32_t const words = static_cast<uint32_t>(bytes / sizeof(uint4));
+  upload_kernel<<<1, 256, 0, stream>>>(block, static_cast<uint4*>(out), words);
+  check(cudaGetLastError(), "radio scratch upload");
+}
+
+// Whether every observer seen shares one destination row (the ingest then
+// writes each track's source terms).
+struct SharedDestination {
+  bool any = false, shared = true;
+  c8r::Destination row{};
+  void see(ObserverCache const& o) {
+    c8r::Destination d{};
+    if (!c8r::shared_destination(&o, 1, d)) return;
+    if (!any) {
+      row = d;
+      any = true;
+    } else {
+      ObserverCache pair[2] = {o, o};
+      pair[1].dest_height = row.height;
+      pair[1].dest_index = row.index;
+      pair[1].dest_n = row.n;
+      pair[1].dest_integral = row.integral;
+      shared = shared && c8r::shared_destination(pair, 2, d);
+    }
+  }
+};
+
+// The accumulator's per-observer constants (make_observer_cache), built a
+// block at a time on the host and uploaded by value.
 void upload_observers(c8r_config const& config, int algorithm, ObserverCache* device_out,
-                      std::size_t& bins, cudaStream_t stream) {
+                      std::size_t& bins, SharedDestination& destination, cudaStream_t stream) {
+  static_assert(sizeof(ObserverCache) % sizeof(uint4) == 0, "observer constants in 16-byte words");
   c8r_observer_snapshot const* snapshots = algorithm == 0 ? config.coreas_observers : config.zhs_observers;
   std::size_t const count = algorithm == 0 ? config.coreas_observer_count : config.zhs_observer_count;
   auto const& p = config.propagation;
   bool const homogeneous = p.homogeneous_refractive_index > 0.;
   bool const fixed = config.deterministic != 0;
   double const limit = config.fixed_point_field_limit_v_per_m;
-  constexpr std::size_t kBlock = 32;
-  ObserverCache block[kBlock];
+  constexpr std::size_t kBlock = kUploadBytes / sizeof(ObserverCache);
+  UploadBlock block;
   std::size_t offset = 0;
   for (std::size_t first = 0; first < count; first += kBlock) {
     std::size_t const n = std::min(kBlock, count - first);
     for (std::size_t k = 0; k < n; ++k) {
       c8r_observer_snapshot const& s = snapshots[first + k];
-      block[k] = c8r::make_observer_cache(
+      ObserverCache const cache = c8r::make_observer_cache(
           s, algorithm, homogeneous, p.minimum_height_m, p.inverse_step_per_m,
           [&](uint64_t i) { return make_double2(p.refractivity[i], p.integrated_refractivity[i]); },
           fixed, limit, config.count_samples != 0, offset);
+      destination.see(cache);
+      std::memcpy(reinterpret_cast<unsigned char*>(block.words) + k * sizeof(ObserverCache), &cache,
+                  sizeof cache);
       offset += static_cast<std::size_t>(s.number_of_bins);
     }
-    // pageable source: the copy has read `block` when the call returns
-    check(cudaMemcpyAsync(device_out + first, block, n * sizeof(ObserverCache), cudaMemcpyHostToDevice,
-                          stream),
-          "radio observer upload");
+    upload(block, device_out + first, n * sizeof(ObserverCache), stream);
   }
   bins = offset;
+}
+
+// The {n-1, integral} table interleaved from the caller's two arrays.
+void upload_table(c8r_propagation_snapshot const& p, double2* device_out, cudaStream_t stream) {
+  constexpr std::size_t kBlock = kUploadBytes / sizeof(double2);
+  UploadBlock block;
+  auto* entries = reinterpret_cast<double2*>(block.words);
+  for (std::size_t first = 0; first < p.table_size; first += kBlock) {
+    std::size_t const n = std::min<std::size_t>(kBlock, p.table_size - first);
+    for (std::size_t k = 0; k < n; ++k)
+      entries[k] = make_double2(p.refractivity[first + k], p.integrated_refractivity[first + k]);
+    upload(block, device_out + first, n * sizeof(double2), stream);
+  }
 }
 
 void accumulate_no_alloc(c8r_config const& config, c8r_lepton_transport_record const* records,
@@ -161,6 +220,9 @@ void accumulate_no_alloc(c8r_config const& config, c8r_lepton_transport_record c
                             std::to_string(kMaxTableEntries) + " entries does not fit its static scratch");
   if ((on[0] && observers[0] && coreas_traces == nullptr) || (on[1] && observers[1] && zhs_traces == nullptr))
     throw std::invalid_argument("null device radio trace output");
+
+  // nothing to project: no device work at all
+  if (count == 0 || observers[0] + observers[1] == 0) return;
 
   DeviceSetup const& dev = setup_current_device();
   unsigned char* const base = dev.scratch;
@@ -191,23 +253,18 @@ void accumulate_no_alloc(c8r_config const& config, c8r_lepton_transport_record c
   prop.table_size = p.table_size;
   prop.refinement = config.zhs_subtrack_refinement;
   if (!homogeneous) {
-    check(cudaMemcpy2DAsync(&table[0].x, sizeof(double2), p.refractivity, sizeof(double), sizeof(double),
-                            p.table_size, cudaMemcpyHostToDevice, stream),
-          "radio table upload");
-    check(cudaMemcpy2DAsync(&table[0].y, sizeof(double2), p.integrated_refractivity, sizeof(double),
-                            sizeof(double), p.table_size, cudaMemcpyHostToDevice, stream),
-          "radio table upload");
+    upload_table(p, table, stream);
     prop.table = table;
   }
   std::size_t bins[2] = {0, 0};
   uint64_t largest = 0;
+  SharedDestination destination;
   for (int a = 0; a < 2; ++a) {
     if (!observers[a]) continue;
-    upload_observers(config, a, caches + (a == 0 ? 0 : observers[0]), bins[a], stream);
+    upload_observers(config, a, caches + (a == 0 ? 0 : observers[0]), bins[a], destination, stream);
     c8r_observer_snapshot const* s = a == 0 ? config.coreas_observers : config.zhs_observers;
     for (std::size_t i = 0; i < observers[a]; ++i) largest = std::max<uint64_t>(largest, s[i].number_of_bins);
   }
-  if (count == 0 || observers[0] + observers[1] == 0) return;
 
   bool const fixed = config.deterministic != 0;
   c8r::Precision const precision =
@@ -238,6 +295,11 @@ void accumulate_no_alloc(c8r_config const& config, c8r_lepton_transport_record c
   ev.window = window;
   ev.first_track = 0;
   ev.last_track = ~0ull;
+  c8r::IngestTerms terms{};
+  terms.enabled = destination.any && destination.shared ? 1 : 0;
+  terms.propagation = prop;
+  terms.destination = destination.row;
+  ev.precomputed = static_cast<uint32_t>(terms.enabled);
 
   // records in chunks of at most kTrackCapacity: ingest into the scratch
   // kinematics, then one persistent launch per algorithm over the chunk
@@ -245,7 +307,7 @@ void accumulate_no_alloc(c8r_config const& config, c8r_lepton_transport_record c
     std::size_t const n = std::min(kTrackCapacity, count - begin);
     check(cudaMemsetAsync(slot, 0, sizeof(unsigned long long), stream), "radio scratch clear");
     check(c8r::launch_ingest(records + begin, n, tracks, kTrackCapacity, slot, event_counters,
-                             config.track_diagnostics != 0, stream),
+                             config.track_diagnostics != 0, terms, stream),
           "radio ingest launch");
     std::size_t const ctas_total = static_cast<std::size_t>(dev.sms) * 2;
     std::size_t const per_item = observers[0] + observers[1];

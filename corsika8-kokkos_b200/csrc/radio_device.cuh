@@ -71,12 +71,19 @@ struct Track {
   double length, beta_module, constant;
 };
 
-// Track workspace: one 128-byte record of 16 doubles per track (start xyz,
-// end xyz, t_start, t_end, beta xyz, length, |beta|, charge constant, two
-// spare), read by each thread with eight 16-byte vector loads.
+// Track workspace: one 192-byte record of 24 doubles per track.  The first
+// 16: start xyz, end xyz, t_start, t_end, beta xyz, length, |beta|, charge
+// constant, n_dst at the start point, one spare.  When every observer of the
+// event shares one destination row (SourceTerms below), the last 8 hold the
+// propagation terms of four source points, precomputed at ingest: start,
+// end, the ZHS segment midpoint (start + (start + (end - start))) / 2, and
+// the CoREAS near-cone midpoint (start + end) / 2 -- each as (factor, n_src).
 enum TrackField : int {
-  kSx = 0, kSy, kSz, kEx, kEy, kEz, kTs, kTe, kBx, kBy, kBz, kLen, kBmod, kConst, kTrackDoubles = 16
+  kSx = 0, kSy, kSz, kEx, kEy, kEz, kTs, kTe, kBx, kBy, kBz, kLen, kBmod, kConst, kNdstStart, kSpare,
+  kFactorStart, kNsrcStart, kFactorEnd, kNsrcEnd, kFactorMidZhs, kNsrcMidZhs, kFactorMidCoreas,
+  kNsrcMidCoreas, kTrackDoubles
 };
+static_assert(kTrackDoubles == 24, "192-byte track records");
 
 struct Path {
   double time, n_src, n_dst, dist, kx, ky, kz;
@@ -121,14 +128,76 @@ __device__ __forceinline__ double doppler(double index, double bx, double by, do
   return (1. - product) - product_error;
 }
 
-// propagate, RadioProjection.inl:170-238.  kTime = false skips the refractive
-// index and travel time (the Fraunhofer midpoint uses only k and distance).
-// kApproxDirection = true returns k = d * RN(1/|d|): each component within
-// 3.01 u |k| of the reference's RN(d/|d|) (u = 2^-53); distance, refractive
-// indices and travel time are exact in both forms.
+// The destination row of propagate (RadioProjection.inl:184-192) as the
+// projection sees it: the observer's height in table steps, its table index,
+// n and integrated refractivity there.  Observers with the same four values
+// give the same source terms for a source point.
+struct Destination {
+  double height;
+  uint64_t index;
+  double n;
+  double integral;
+};
+
+__device__ __forceinline__ Destination destination_of(ObserverCache const& o) {
+  return Destination{o.dest_height, o.dest_index, o.dest_n, o.dest_integral};
+}
+inline Destination destination_of_host(ObserverCache const& o) {
+  return Destination{o.dest_height, o.dest_index, o.dest_n, o.dest_integral};
+}
+
+// The part of propagate (RadioProjection.inl:170-238) that depends on the
+// source's height and the destination row only: the travel time is
+// factor * |d| / c, with factor = 1 + (I_src - I_dst) / height from the table
+// (n for a homogeneous medium), and the refractive indices at both ends.
+struct SourceTerms {
+  double factor, n_src, n_dst;
+};
+
+__device__ __forceinline__ SourceTerms source_terms(Propagation const& p, Destination const& d, double sz) {
+  if (p.homogeneous > 0.) return SourceTerms{p.homogeneous, p.homogeneous, p.homogeneous};
+  double const sh = (sz - p.min_height) * p.inv_step;
+  double const dh = d.height;
+  uint64_t const last = p.table_size - 1;
+  double n_src = 1., i_src = 1., n_dst = d.n, height = 1.;
+  if (sh + 0.5 >= static_cast<double>(last)) {
+    double2 const t = __ldg(p.table + last);
+    n_src = t.x + p.slope_n_upper * fabs((sz - p.max_height) * p.inv_step) + 1.;
+    i_src = t.y + p.slope_i_upper * fabs(p.max_height - sz);
+    height = sh - dh;
+  } else if (sh + 0.5 < static_cast<double>(last) && sh > 0.) {
+    uint64_t const si = static_cast<uint64_t>(sh + 0.5);
+    double2 const t = __ldg(p.table + si);
+    n_src = t.x + 1.;
+    i_src = t.y;
+    height = static_cast<double>(static_cast<int64_t>(si) - static_cast<int64_t>(d.index)) * p.step;
+    if (height == 0.) height = 1.;
+  } else if (sh == 0.) {
+    n_src = 1.;
+    n_dst = 1.;
+    i_src = __ldg(p.table).y;
+    height = dh - sh;
+  } else {
+    double2 const t0 = __ldg(p.table);
+    n_src = t0.x + p.slope_n_lower * fabs(sh) + 1.;
+    i_src = t0.y + p.slope_i_lower * fabs(sh);
+    n_dst = 1.;
+    height = dh - fabs(sh);
+  }
+  return SourceTerms{1. + (i_src - d.integral) / height, n_src, n_dst};
+}
+
+// propagate, RadioProjection.inl:170-238, given the source terms of the
+// point: the reference's (1 + (I_src - I_dst) / height) * dist / c with the
+// parenthesised factor taken from `st` (the same IEEE value), or n dist / c.
+// kTime = false skips the refractive index and travel time (the Fraunhofer
+// midpoint uses only k and distance).  kApproxDirection = true returns
+// k = d * RN(1/|d|): each component within 3.01 u |k| of the reference's
+// RN(d/|d|) (u = 2^-53); distance, refractive indices and travel time are
+// exact in both forms.
 template <bool kTime, bool kApproxDirection = false>
-__device__ __forceinline__ Path propagate(Propagation const& p, ObserverCache const& o,
-                                          double sx, double sy, double sz) {
+__device__ __forceinline__ Path propagate_with(SourceTerms const& st, ObserverCache const& o,
+                                               double sx, double sy, double sz) {
   Path r;
   double const dx = o.px - sx, dy = o.py - sy, dz = o.pz - sz;
   double const dist = sqrt(dx * dx + dy * dy + dz * dz);
@@ -144,44 +213,19 @@ __device__ __forceinline__ Path propagate(Propagation const& p, ObserverCache co
   }
   r.dist = dist;
   if (!kTime) return r;
-  if (p.homogeneous > 0.) {
-    r.time = p.homogeneous * dist / kSpeedOfLight;
-    r.n_src = r.n_dst = p.homogeneous;
-    return r;
-  }
-  double const sh = (sz - p.min_height) * p.inv_step;
-  double const dh = o.dest_height;
-  uint64_t const last = p.table_size - 1;
-  double n_src = 1., i_src = 1., n_dst = o.dest_n, height = 1.;
-  if (sh + 0.5 >= static_cast<double>(last)) {
-    double2 const t = __ldg(p.table + last);
-    n_src = t.x + p.slope_n_upper * fabs((sz - p.max_height) * p.inv_step) + 1.;
-    i_src = t.y + p.slope_i_upper * fabs(p.max_height - sz);
-    height = sh - dh;
-  } else if (sh + 0.5 < static_cast<double>(last) && sh > 0.) {
-    uint64_t const si = static_cast<uint64_t>(sh + 0.5);
-    double2 const t = __ldg(p.table + si);
-    n_src = t.x + 1.;
-    i_src = t.y;
-    height = static_cast<double>(static_cast<int64_t>(si) - static_cast<int64_t>(o.dest_index)) *
-             p.step;
-    if (height == 0.) height = 1.;
-  } else if (sh == 0.) {
-    n_src = 1.;
-    n_dst = 1.;
-    i_src = __ldg(p.table).y;
-    height = dh - sh;
-  } else {
-    double2 const t0 = __ldg(p.table);
-    n_src = t0.x + p.slope_n_lower * fabs(sh) + 1.;
-    i_src = t0.y + p.slope_i_lower * fabs(sh);
-    n_dst = 1.;
-    height = dh - fabs(sh);
-  }
-  r.time = (1. + (i_src - o.dest_integral) / height) * dist / kSpeedOfLight;
-  r.n_src = n_src;
-  r.n_dst = n_dst;
+  r.time = st.factor * dist / kSpeedOfLight;
+  r.n_src = st.n_src;
+  r.n_dst = st.n_dst;
   return r;
+}
+
+// propagate, RadioProjection.inl:170-238: the source terms looked up in the
+// table for this observer, then the path.
+template <bool kTime, bool kApproxDirection = false>
+__device__ __forceinline__ Path propagate(Propagation const& p, ObserverCache const& o,
+                                          double sx, double sy, double sz) {
+  SourceTerms const st = kTime ? source_terms(p, destination_of(o), sz) : SourceTerms{0., 0., 0.};
+  return propagate_with<kTime, kApproxDirection>(st, o, sx, sy, sz);
 }
 
 // propagate (RadioProjection.inl:170-238) for the filtered decisions of the
@@ -202,10 +246,10 @@ struct FastPath {
   bool ok;
 };
 
-__device__ __forceinline__ FastPath propagate_fast(Propagation const& p, ObserverCache const& o,
-                                                   double sx, double sy, double sz) {
+__device__ __forceinline__ FastPath propagate_fast_with(SourceTerms const& st, double ox, double oy, double oz,
+                                                        double sx, double sy, double sz) {
   FastPath r;
-  double const dx = o.px - sx, dy = o.py - sy, dz = o.pz - sz;
+  double const dx = ox - sx, dy = oy - sy, dz = oz - sz;
   double const s2 = dx * dx + dy * dy + dz * dz;
   r.ok = s2 >= 0x1p-100 && s2 <= 0x1p100;
   double y = static_cast<double>(rsqrtf(static_cast<float>(r.ok ? s2 : 1.)));
@@ -221,48 +265,17 @@ __device__ __forceinline__ FastPath propagate_fast(Propagation const& p, Observe
   r.kz = dz * y;
   r.dist = dist;
   constexpr double kInverseC = 1. / kSpeedOfLight;
-  if (p.homogeneous > 0.) {
-    r.time = p.homogeneous * dist * kInverseC;
-    r.n_src = r.n_dst = p.homogeneous;
-    r.time_err = 0x1p-48 * fabs(r.time);
-    r.ok = r.ok && r.time_err < 1.e300;
-    return r;
-  }
-  double const sh = (sz - p.min_height) * p.inv_step;
-  double const dh = o.dest_height;
-  uint64_t const last = p.table_size - 1;
-  double n_src = 1., i_src = 1., n_dst = o.dest_n, height = 1.;
-  if (sh + 0.5 >= static_cast<double>(last)) {
-    double2 const t = __ldg(p.table + last);
-    n_src = t.x + p.slope_n_upper * fabs((sz - p.max_height) * p.inv_step) + 1.;
-    i_src = t.y + p.slope_i_upper * fabs(p.max_height - sz);
-    height = sh - dh;
-  } else if (sh + 0.5 < static_cast<double>(last) && sh > 0.) {
-    uint64_t const si = static_cast<uint64_t>(sh + 0.5);
-    double2 const t = __ldg(p.table + si);
-    n_src = t.x + 1.;
-    i_src = t.y;
-    height = static_cast<double>(static_cast<int64_t>(si) - static_cast<int64_t>(o.dest_index)) *
-             p.step;
-    if (height == 0.) height = 1.;
-  } else if (sh == 0.) {
-    n_src = 1.;
-    n_dst = 1.;
-    i_src = __ldg(p.table).y;
-    height = dh - sh;
-  } else {
-    double2 const t0 = __ldg(p.table);
-    n_src = t0.x + p.slope_n_lower * fabs(sh) + 1.;
-    i_src = t0.y + p.slope_i_lower * fabs(sh);
-    n_dst = 1.;
-    height = dh - fabs(sh);
-  }
-  r.time = (1. + (i_src - o.dest_integral) / height) * dist * kInverseC;
-  r.n_src = n_src;
-  r.n_dst = n_dst;
+  r.time = st.factor * dist * kInverseC;
+  r.n_src = st.n_src;
+  r.n_dst = st.n_dst;
   r.time_err = 0x1p-48 * fabs(r.time);
   r.ok = r.ok && r.time_err < 1.e300;  // false for infinite or NaN times
   return r;
+}
+
+__device__ __forceinline__ FastPath propagate_fast(Propagation const& p, ObserverCache const& o,
+                                                   double sx, double sy, double sz) {
+  return propagate_fast_with(source_terms(p, destination_of(o), sz), o.px, o.py, o.pz, sx, sy, sz);
 }
 
 // separate_same_bin_endpoints, RadioProjection.inl:303-336.

@@ -19,6 +19,8 @@
 
 #include <cuda_runtime.h>
 
+#include <cstring>
+
 #include "../../include/c8radio.h"
 
 namespace c8r {
@@ -128,6 +130,25 @@ __device__ __forceinline__ void spillf3(double* r0, double* r1, double* r2, doub
   atomicAdd(r2, z);
 }
 
+// Adds to the shared-memory window through its shared-space address.  The
+// window pointer reaches the sinks through structs and out-of-line calls, so
+// plain atomicAdd on it compiles to generic atomics; these name the shared
+// state space.  No memory clobber: the window is read only after a barrier.
+__device__ __forceinline__ unsigned shared_address(void const* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void shared_red_add(unsigned long long* p, unsigned long long v) {
+  asm volatile("red.shared.add.u64 [%0], %1;" ::"r"(shared_address(p)), "l"(v));
+}
+__device__ __forceinline__ unsigned long long shared_atom_add(unsigned long long* p, unsigned long long v) {
+  unsigned long long previous;
+  asm volatile("atom.shared.add.u64 %0, [%1], %2;" : "=l"(previous) : "r"(shared_address(p)), "l"(v));
+  return previous;
+}
+__device__ __forceinline__ void shared_red_add(double* p, double v) {
+  asm volatile("red.shared.add.f64 [%0], %1;" ::"r"(shared_address(p)), "d"(v));
+}
+
 // Shared-memory window of `width` bins starting at bin 0 (rows X|Y|Z), with
 // bins past the window spilled to the global rows.
 struct WindowSink {
@@ -146,16 +167,16 @@ struct WindowSink {
       return spill3(row[0] + bin, row[1] + bin, row[2] + bin, x, y, z, ox, oy, oz);
     unsigned long long* const w = win + bin;
     if (unchecked) {
-      if (ox) atomicAdd(w, static_cast<unsigned long long>(x));
-      if (oy) atomicAdd(w + width, static_cast<unsigned long long>(y));
-      if (oz) atomicAdd(w + 2 * width, static_cast<unsigned long long>(z));
+      if (ox) shared_red_add(w, static_cast<unsigned long long>(x));
+      if (oy) shared_red_add(w + width, static_cast<unsigned long long>(y));
+      if (oz) shared_red_add(w + 2 * width, static_cast<unsigned long long>(z));
       bound += mag;
       return ox && oy && oz;
     }
-    unsigned long long const px = ox ? atomicAdd(w, static_cast<unsigned long long>(x)) : 0ull;
-    unsigned long long const py = oy ? atomicAdd(w + width, static_cast<unsigned long long>(y)) : 0ull;
+    unsigned long long const px = ox ? shared_atom_add(w, static_cast<unsigned long long>(x)) : 0ull;
+    unsigned long long const py = oy ? shared_atom_add(w + width, static_cast<unsigned long long>(y)) : 0ull;
     unsigned long long const pz =
-        oz ? atomicAdd(w + 2 * width, static_cast<unsigned long long>(z)) : 0ull;
+        oz ? shared_atom_add(w + 2 * width, static_cast<unsigned long long>(z)) : 0ull;
     return ox && oy && oz && no_overflow3(px, x, py, y, pz, z);
   }
   __device__ __forceinline__ void addf3(uint64_t bin, double x, double y, double z) {
@@ -164,9 +185,9 @@ struct WindowSink {
       return;
     }
     double* const w = fwin + bin;
-    atomicAdd(w, x);
-    atomicAdd(w + width, y);
-    atomicAdd(w + 2 * width, z);
+    shared_red_add(w, x);
+    shared_red_add(w + width, y);
+    shared_red_add(w + 2 * width, z);
   }
 };
 
@@ -347,12 +368,15 @@ __device__ __forceinline__ void coreas_pair(Track const& t, Propagation const& p
 }
 
 // The propagation of the filtered paths: propagate_fast when kFast, else the
-// exact propagate (time_err 0).
-template <bool kFast>
+// exact propagate (time_err 0).  kPre: the point's source terms are `pre`
+// (precomputed at ingest), else they are looked up in the table.
+template <bool kFast, bool kPre = false>
 __device__ __forceinline__ FastPath filtered_path(Propagation const& p, ObserverCache const& o,
-                                                  double x, double y, double z) {
-  if (kFast) return propagate_fast(p, o, x, y, z);
-  Path const e = propagate<true>(p, o, x, y, z);
+                                                  double x, double y, double z,
+                                                  SourceTerms const& pre = SourceTerms{}) {
+  SourceTerms const st = kPre ? pre : source_terms(p, destination_of(o), z);
+  if (kFast) return propagate_fast_with(st, o.px, o.py, o.pz, x, y, z);
+  Path const e = propagate_with<true>(st, o, x, y, z);
   return FastPath{e.time, e.n_src, e.n_dst, e.dist, e.kx, e.ky, e.kz, 0., true};
 }
 
@@ -369,11 +393,14 @@ __device__ __forceinline__ FastPath filtered_path(Propagation const& p, Observer
 // doppler < 1e-9) are taken here only when that bound cannot move them, and
 // pairs with |doppler| < 1e-6 are left to the exact evaluation.  Sample times
 // are exact, so bins are the reference's.
-template <bool kFixed, bool kFilter, class Amp, class Sink>
+template <bool kFixed, bool kFilter, bool kPre, class Amp, class Sink>
 __device__ __forceinline__ bool coreas_common(Track const& t, Propagation const& p,
-                                              ObserverCache const& o, Sink& sink, Counts& c) {
-  Path const ps = propagate<true, kFilter>(p, o, t.sx, t.sy, t.sz);
-  Path const pe = propagate<true, kFilter>(p, o, t.ex, t.ey, t.ez);
+                                              ObserverCache const& o, Sink& sink, Counts& c,
+                                              SourceTerms const& pre_start, SourceTerms const& pre_end) {
+  Path const ps = kPre ? propagate_with<true, kFilter>(pre_start, o, t.sx, t.sy, t.sz)
+                       : propagate<true, kFilter>(p, o, t.sx, t.sy, t.sz);
+  Path const pe = kPre ? propagate_with<true, kFilter>(pre_end, o, t.ex, t.ey, t.ez)
+                       : propagate<true, kFilter>(p, o, t.ex, t.ey, t.ez);
   double pre, post;
   if (kFilter) {
     pre = 1. - ps.n_src * (t.bx * ps.kx + t.by * ps.ky + t.bz * ps.kz);
@@ -610,15 +637,16 @@ struct StagedSegment<double> {
 // segment needs the per-index binning or (kFilter) an exact evaluation, or
 // when the trace has 2^26 bins or more (staged counts then stay far inside 32
 // bits per warp).
-template <bool kFilter, class Amp>
+template <bool kFilter, class Amp, bool kPre = false>
 __device__ __forceinline__ bool zhs_stage(double p1x, double p1y, double p1z, double p2x,
                                           double p2y, double p2z, double t1, double t2,
                                           Track const& t, Propagation const& p,
                                           ObserverCache const& o, bool subdivided,
-                                          StagedSegment<Amp>& out) {
+                                          StagedSegment<Amp>& out,
+                                          SourceTerms const& pre = SourceTerms{}) {
   if (!(o.bins_d < 67108864.0)) return false;
   double const mx = (p1x + p2x) * 0.5, my = (p1y + p2y) * 0.5, mz = (p1z + p2z) * 0.5;
-  FastPath const path = filtered_path<kFilter>(p, o, mx, my, mz);
+  FastPath const path = filtered_path<kFilter, kPre>(p, o, mx, my, mz, pre);
   if (kFilter && !path.ok) return false;
   double const bk = t.bx * path.kx + t.by * path.ky + t.bz * path.kz;
   double const nbk = path.n_src * bk;
@@ -841,10 +869,10 @@ __device__ __forceinline__ void zhs_pair(Track const& t, Propagation const& p,
 // 1e-12 K (cross-product cancellation, the FP32 roundings and the approximate
 // reciprocals; used with margins of 2.3x and more), so an estimate surely
 // below 1 decides "one segment" exactly as the reference does.
-template <bool kFilter, class Amp>
+template <bool kFilter, bool kPre, class Amp>
 __device__ __forceinline__ bool zhs_common(Track const& t, Propagation const& p,
                                            ObserverCache const& o, Counts& c,
-                                           StagedSegment<Amp>& seg) {
+                                           StagedSegment<Amp>& seg, SourceTerms const& pre_mid) {
   if (p.refinement != 1u) return false;
   double const mx = (t.sx + t.ex) * 0.5, my = (t.sy + t.ey) * 0.5, mz = (t.sz + t.ez) * 0.5;
   if (kFilter) {
@@ -872,9 +900,9 @@ __device__ __forceinline__ bool zhs_common(Track const& t, Propagation const& p,
     double const fraunhofer = s2 * t.length * t.length / pm.dist / o.wavelength * 2. * kPi;
     if (fraunhofer > 1.) return false;
   }
-  if (!zhs_stage<kFilter, Amp>(t.sx, t.sy, t.sz, t.sx + (t.ex - t.sx), t.sy + (t.ey - t.sy),
-                               t.sz + (t.ez - t.sz), t.ts, t.ts + (t.te - t.ts), t, p, o, false,
-                               seg))
+  if (!zhs_stage<kFilter, Amp, kPre>(t.sx, t.sy, t.sz, t.sx + (t.ex - t.sx), t.sy + (t.ey - t.sy),
+                                     t.sz + (t.ez - t.sz), t.ts, t.ts + (t.te - t.ts), t, p, o, false,
+                                     seg, pre_mid))
     return false;
   c.subtracks += 1ull;
   return true;
@@ -887,6 +915,28 @@ __device__ __forceinline__ Track load_track(const double* __restrict__ base, uin
   double2 const* r = reinterpret_cast<double2 const*>(base + i * kTrackDoubles);
   double2 const a = __ldg(r + 0), b = __ldg(r + 1), c = __ldg(r + 2), d = __ldg(r + 3);
   double2 const e = __ldg(r + 4), f = __ldg(r + 5), g = __ldg(r + 6);
+  Track t;
+  t.sx = a.x;
+  t.sy = a.y;
+  t.sz = b.x;
+  t.ex = b.y;
+  t.ey = c.x;
+  t.ez = c.y;
+  t.ts = d.x;
+  t.te = d.y;
+  t.bx = e.x;
+  t.by = e.y;
+  t.bz = f.x;
+  t.length = f.y;
+  t.beta_module = g.x;
+  t.constant = g.y;
+  return t;
+}
+
+// A track staged in shared memory (plain loads: __ldg reads the global space only).
+__device__ __forceinline__ Track load_staged_track(double const* base, unsigned i) {
+  double2 const* r = reinterpret_cast<double2 const*>(base + i * kTrackDoubles);
+  double2 const a = r[0], b = r[1], c = r[2], d = r[3], e = r[4], f = r[5], g = r[6];
   Track t;
   t.sx = a.x;
   t.sy = a.y;
@@ -980,7 +1030,8 @@ struct ColumnSource {
 template <class Source>
 __global__ void __launch_bounds__(256) ingest_kernel(
     const __grid_constant__ Source src, uint64_t count, double* __restrict__ tracks, uint64_t stride,
-    unsigned long long* slot, DeviceCounters* counters, int diagnostics) {
+    unsigned long long* slot, DeviceCounters* counters, int diagnostics,
+    const __grid_constant__ IngestTerms terms) {
   uint64_t const i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   bool valid = false;
   Track t;
@@ -1028,7 +1079,25 @@ __global__ void __launch_bounds__(256) ingest_kernel(
     r[4] = make_double2(t.bx, t.by);
     r[5] = make_double2(t.bz, t.length);
     r[6] = make_double2(t.beta_module, t.constant);
-    r[7] = make_double2(0., 0.);
+    if (terms.enabled) {
+      // the source points of the windowed kernels' common paths, with the
+      // reference's own arithmetic: the ZHS segment of an undivided track ends
+      // at start + (end - start) (RadioProjection.inl:505-512), the CoREAS
+      // near-cone midpoint is (start + end) / 2 (:357-359)
+      Propagation const& p = terms.propagation;
+      Destination const& d = terms.destination;
+      SourceTerms const s = source_terms(p, d, t.sz);
+      SourceTerms const e = source_terms(p, d, t.ez);
+      SourceTerms const mz = source_terms(p, d, (t.sz + (t.sz + (t.ez - t.sz))) * 0.5);
+      SourceTerms const mc = source_terms(p, d, (t.sz + t.ez) * 0.5);
+      r[7] = make_double2(s.n_dst, 0.);
+      r[8] = make_double2(s.factor, s.n_src);
+      r[9] = make_double2(e.factor, e.n_src);
+      r[10] = make_double2(mz.factor, mz.n_src);
+      r[11] = make_double2(mc.factor, mc.n_src);
+    } else {
+      r[7] = make_double2(0., 0.);
+    }
   }
   if (lane == 0 && ballot) atomicAdd(&counters->valid_tracks, static_cast<unsigned long long>(__popc(ballot)));
   if (!diagnostics) return;
@@ -1148,6 +1217,81 @@ __global__ void __launch_bounds__(256) direct_kernel(const __grid_constant__ Eve
         sink.frow[r] = kFixed ? nullptr : ev.floating[1] + r * ev.total_bins[1] + o.offset;
       }
       zhs_pair<kFixed, false, Amp>(t, ev.propagation, o, sink, c);
+    }
+  }
+  flush_counts(c, ev.counters);
+}
+
+// ---------------------------------------------------------------- tiled
+// The reference's large-batch launch shape (RadioTileProjection,
+// RadioAccumulator.inl:13-85, launched by project(), :699-847, for batches
+// of 16384 tracks or more on a GPU): one 256-thread CTA per tile of
+// kTileTracks tracks x kTileObservers observers, the tile's track kinematics
+// and observer constants staged in shared memory, one thread per pair (lane
+// l takes track l / 32 at observer l % 32, so a warp holds one track at 32
+// observers), every sample a checked 64-bit global atomic.  Tiles are taken
+// by a grid-stride loop over track tile x observer tile.
+constexpr int kTileTracks = 8;      // RadioAccumulator.hpp:61 (TrackTileSize)
+constexpr int kTileObservers = 32;  // RadioAccumulator.hpp:62 (ObserverTileSize)
+constexpr int kTileThreads = kTileTracks * kTileObservers;
+static_assert(sizeof(ObserverCache) % sizeof(double2) == 0, "observer constants in 16-byte words");
+
+template <bool kFixed, class Amp, bool kCoreas, bool kZhs>
+__global__ void __launch_bounds__(kTileThreads) tiled_kernel(const __grid_constant__ EventPlan ev,
+                                                              uint64_t track_tiles) {
+  __shared__ __align__(16) double tracks[kTileTracks * kTrackDoubles];
+  __shared__ ObserverCache observers[2][kTileObservers];
+  uint64_t const valid = *ev.valid_tracks;
+  uint32_t const observer_count =
+      ev.observer_count[0] > ev.observer_count[1] ? ev.observer_count[0] : ev.observer_count[1];
+  uint64_t const observer_tiles = (observer_count + kTileObservers - 1) / kTileObservers;
+  uint64_t const tiles = track_tiles * observer_tiles;
+  unsigned const track_lane = threadIdx.x / kTileObservers;
+  unsigned const observer_lane = threadIdx.x % kTileObservers;
+  Counts c;
+  for (uint64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    uint64_t const track_base = (tile / observer_tiles) * kTileTracks;
+    uint64_t const observer_base = (tile % observer_tiles) * kTileObservers;
+    __syncthreads();  // the previous tile's reads are done
+    for (unsigned i = threadIdx.x; i < kTileTracks * kTrackDoubles / 2; i += blockDim.x) {
+      uint64_t const row = track_base + i / (kTrackDoubles / 2);
+      reinterpret_cast<double2*>(tracks)[i] =
+          row < valid ? __ldg(reinterpret_cast<double2 const*>(ev.tracks) + track_base * (kTrackDoubles / 2) + i)
+                      : make_double2(0., 0.);
+    }
+    constexpr unsigned kWords = sizeof(ObserverCache) / sizeof(double2);
+    for (int a = 0; a < 2; ++a) {
+      if (!(a == 0 ? kCoreas : kZhs)) continue;
+      for (unsigned i = threadIdx.x; i < kTileObservers * kWords; i += blockDim.x) {
+        uint64_t const index = observer_base + i / kWords;
+        if (index < ev.observer_count[a])
+          reinterpret_cast<double2*>(observers[a])[i] =
+              __ldg(reinterpret_cast<double2 const*>(ev.observers[a] + observer_base) + i);
+      }
+    }
+    __syncthreads();
+    uint64_t const ti = track_base + track_lane;
+    uint64_t const oi = observer_base + observer_lane;
+    if (ti < valid) {
+      Track const t = load_staged_track(tracks, track_lane);
+      if (kCoreas && oi < ev.observer_count[0]) {
+        ObserverCache const& o = observers[0][observer_lane];
+        GlobalSink sink;
+        for (int r = 0; r < 3; ++r) {
+          sink.row[r] = kFixed ? ev.fixed[0] + r * ev.total_bins[0] + o.offset : nullptr;
+          sink.frow[r] = kFixed ? nullptr : ev.floating[0] + r * ev.total_bins[0] + o.offset;
+        }
+        coreas_pair<kFixed, Amp>(t, ev.propagation, o, sink, c);
+      }
+      if (kZhs && oi < ev.observer_count[1]) {
+        ObserverCache const& o = observers[1][observer_lane];
+        GlobalSink sink;
+        for (int r = 0; r < 3; ++r) {
+          sink.row[r] = kFixed ? ev.fixed[1] + r * ev.total_bins[1] + o.offset : nullptr;
+          sink.frow[r] = kFixed ? nullptr : ev.floating[1] + r * ev.total_bins[1] + o.offset;
+        }
+        zhs_pair<kFixed, false, Amp>(t, ev.propagation, o, sink, c);
+      }
     }
   }
   flush_counts(c, ev.counters);
@@ -1286,7 +1430,23 @@ __device__ __noinline__ Counts coreas_drain_pair(const double* __restrict__ trac
   return c;
 }
 
-template <bool kFixed, class Amp, int kAlgorithm>
+// The precomputed source terms of a track's common path (kTrackDoubles):
+// CoREAS start and end (n_dst at the start), ZHS segment midpoint.
+template <int kAlgorithm>
+__device__ __forceinline__ void load_source_terms(const double* __restrict__ base, uint64_t i,
+                                                  SourceTerms& a, SourceTerms& b) {
+  double2 const* r = reinterpret_cast<double2 const*>(base + i * kTrackDoubles);
+  if (kAlgorithm == 0) {
+    double2 const n = __ldg(r + kNdstStart / 2), s = __ldg(r + kFactorStart / 2), e = __ldg(r + kFactorEnd / 2);
+    a = SourceTerms{s.x, s.y, n.x};
+    b = SourceTerms{e.x, e.y, 0.};
+  } else {
+    double2 const m = __ldg(r + kFactorMidZhs / 2);
+    a = SourceTerms{m.x, m.y, 0.};
+  }
+}
+
+template <bool kFixed, class Amp, int kAlgorithm, bool kPre>
 __global__ void __launch_bounds__(kAlgorithm == 1 ? kZhsThreadsMax : kWindowThreadsMax, 1)
     windowed_kernel(const __grid_constant__ WorkPlan plan) {
   extern __shared__ __align__(16) unsigned long long window[];
@@ -1348,11 +1508,15 @@ __global__ void __launch_bounds__(kAlgorithm == 1 ? kZhsThreadsMax : kWindowThre
     Counts const saved = c;
     // Fixed point, whole trace in the window: the window takes unchecked
     // adds, and `c.mag` bounds the sum of |increments| of this thread.  If the
-    // block's bound stays below 2^61 (the FP32 sums are off by a factor below
-    // 1 + 2^-2 for fewer than 2^22 adds a thread), no partial sum of any bin
-    // can have left the int64 range in any order, so no add overflowed; else
-    // the item is run again with checked adds.  Bins past the window and the
-    // flush below are always checked.
+    // block's bound stays below 2^61, no partial sum of any bin can have left
+    // the int64 range in any order, so no add overflowed; else the item is
+    // run again with checked adds.  An FP32 sum of n terms is off by a factor
+    // below 1 + n 2^-24, so a thread's sum counts only while the thread made
+    // fewer than 2^22 adds (factor below 1 + 2^-2); a thread with more (its
+    // deposits since the attempt began: contributions plus failed
+    // conversions, an upper bound of its window adds) sends the item to the
+    // checked run.  Bins past the window and the flush below are always
+    // checked.
     for (int attempt = 0;; ++attempt) {
       if (attempt > 0) {
         for (uint32_t j = threadIdx.x; j < 3 * width; j += blockDim.x) window[j] = 0ull;
@@ -1370,9 +1534,12 @@ __global__ void __launch_bounds__(kAlgorithm == 1 ? kZhsThreadsMax : kWindowThre
         seg.flags = 0u;
         if (i < end) {
           Track const t = load_track(ev.tracks, ev.stride, i);
+          SourceTerms pa{}, pb{};
+          if (kPre) load_source_terms<kAlgorithm>(ev.tracks, i, pa, pb);
           bool const done =
-              kAlgorithm == 0 ? coreas_common<kFixed, kFilter, Amp>(t, ev.propagation, o, sink, c)
-                              : zhs_common<kFilter, Amp>(t, ev.propagation, o, c, seg);
+              kAlgorithm == 0
+                  ? coreas_common<kFixed, kFilter, kPre, Amp>(t, ev.propagation, o, sink, c, pa, pb)
+                  : zhs_common<kFilter, kPre, Amp>(t, ev.propagation, o, c, seg, pa);
           deferred = !done;
         }
         if (kAlgorithm == 1) deposit_staged<kFixed>(staging, seg, o, sink, c);
@@ -1406,12 +1573,16 @@ __global__ void __launch_bounds__(kAlgorithm == 1 ? kZhsThreadsMax : kWindowThre
       }
       __syncthreads();
       if (!sink.unchecked) break;
-      float const thread_bound = static_cast<float>(warp_sum(static_cast<double>(c.mag)));
+      unsigned long long const adds = (c.coreas - saved.coreas) + (c.zhs - saved.zhs) +
+                                      (c.overflows - saved.overflows);
+      double const mine = adds < (1ull << 22) ? static_cast<double>(c.mag) : static_cast<double>(INFINITY);
+      float const thread_bound = static_cast<float>(warp_sum(mine));
       if (lane == 0) atomicAdd(&window_bound, thread_bound);
       __syncthreads();
       float const block_bound = window_bound;
       __syncthreads();
       if (block_bound < 0x1p61f) break;
+      if (threadIdx.x == 0 && plan.reruns) atomicAdd(plan.reruns, 1ull);
       c = saved;
     }
 
@@ -1503,10 +1674,51 @@ cudaError_t direct_dispatch(EventPlan const& ev, uint64_t bound, bool coreas, bo
   return cudaGetLastError();
 }
 
+template <bool kFixed, class Amp>
+cudaError_t tiled_dispatch(EventPlan const& ev, uint64_t bound, bool coreas, bool zhs, cudaStream_t stream) {
+  uint32_t const observers =
+      ev.observer_count[0] > ev.observer_count[1] ? ev.observer_count[0] : ev.observer_count[1];
+  if (bound == 0 || observers == 0) return cudaSuccess;
+  uint64_t const track_tiles = (bound + kTileTracks - 1) / kTileTracks;
+  uint64_t const tiles = track_tiles * ((observers + kTileObservers - 1) / kTileObservers);
+  int device = 0, sms = 148;
+  cudaGetDevice(&device);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  uint64_t const cap = static_cast<uint64_t>(sms) * 64;
+  unsigned const grid = static_cast<unsigned>(tiles < cap ? tiles : cap);
+  if (coreas && zhs)
+    tiled_kernel<kFixed, Amp, true, true><<<grid, kTileThreads, 0, stream>>>(ev, track_tiles);
+  else if (coreas)
+    tiled_kernel<kFixed, Amp, true, false><<<grid, kTileThreads, 0, stream>>>(ev, track_tiles);
+  else if (zhs)
+    tiled_kernel<kFixed, Amp, false, true><<<grid, kTileThreads, 0, stream>>>(ev, track_tiles);
+  return cudaGetLastError();
+}
+
 // window rows | (ZHS) per-warp staging slots
 size_t windowed_smem_bytes(uint32_t window, int algorithm) {
   return static_cast<size_t>(window) * 3 * sizeof(unsigned long long) +
          (algorithm == 1 ? kStagingBytes : 0);
+}
+
+// Every event of the plan carries precomputed source terms.
+bool plan_precomputed(WorkPlan const& plan) {
+  if (plan.event_count == 0) return false;
+  for (uint32_t e = 0; e < plan.event_count; ++e)
+    if (!plan.events[e].precomputed) return false;
+  return true;
+}
+
+template <bool kFixed, class Amp, int kAlgorithm, bool kPre>
+cudaError_t windowed_launch(WorkPlan const& plan, int ctas, int threads, cudaStream_t stream) {
+  size_t const bytes = windowed_smem_bytes(plan.window, kAlgorithm);
+  cudaError_t err = cudaFuncSetAttribute(windowed_kernel<kFixed, Amp, kAlgorithm, kPre>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(bytes));
+  if (err != cudaSuccess) return err;
+  int const block = kAlgorithm == 1 && threads > kZhsThreadsMax ? kZhsThreadsMax : threads;
+  windowed_kernel<kFixed, Amp, kAlgorithm, kPre><<<ctas, block, bytes, stream>>>(plan);
+  return cudaGetLastError();
 }
 
 template <bool kFixed, class Amp, int kAlgorithm>
@@ -1514,14 +1726,8 @@ cudaError_t windowed_dispatch_algorithm(WorkPlan const& plan, int ctas, int thre
                                         cudaStream_t stream) {
   if (plan.deferred == nullptr || plan.deferred_stride < deferred_list_stride(plan))
     return cudaErrorInvalidValue;
-  size_t const bytes = windowed_smem_bytes(plan.window, kAlgorithm);
-  cudaError_t err = cudaFuncSetAttribute(windowed_kernel<kFixed, Amp, kAlgorithm>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(bytes));
-  if (err != cudaSuccess) return err;
-  int const block = kAlgorithm == 1 && threads > kZhsThreadsMax ? kZhsThreadsMax : threads;
-  windowed_kernel<kFixed, Amp, kAlgorithm><<<ctas, block, bytes, stream>>>(plan);
-  return cudaGetLastError();
+  return plan_precomputed(plan) ? windowed_launch<kFixed, Amp, kAlgorithm, true>(plan, ctas, threads, stream)
+                                : windowed_launch<kFixed, Amp, kAlgorithm, false>(plan, ctas, threads, stream);
 }
 
 template <bool kFixed, class Amp>
@@ -1542,8 +1748,11 @@ int ctas_per_sm(int window, int threads) {
       blocks = 0;
     worst = blocks < worst ? blocks : worst;
   };
-  probe(windowed_kernel<kFixed, Amp, 0>, threads, 0);
-  probe(windowed_kernel<kFixed, Amp, 1>, threads > kZhsThreadsMax ? kZhsThreadsMax : threads, 1);
+  probe(windowed_kernel<kFixed, Amp, 0, false>, threads, 0);
+  probe(windowed_kernel<kFixed, Amp, 0, true>, threads, 0);
+  int const zhs_block = threads > kZhsThreadsMax ? kZhsThreadsMax : threads;
+  probe(windowed_kernel<kFixed, Amp, 1, false>, zhs_block, 1);
+  probe(windowed_kernel<kFixed, Amp, 1, true>, zhs_block, 1);
   return worst;
 }
 
@@ -1551,22 +1760,37 @@ int ctas_per_sm(int window, int threads) {
 
 cudaError_t launch_ingest(const c8r_lepton_transport_record* records, uint64_t count,
                           double* tracks, uint64_t stride, unsigned long long* slot,
-                          DeviceCounters* counters, bool diagnostics, cudaStream_t stream) {
+                          DeviceCounters* counters, bool diagnostics, IngestTerms const& terms,
+                          cudaStream_t stream) {
   if (count == 0) return cudaSuccess;
   uint64_t const blocks = (count + 255) / 256;
   ingest_kernel<RecordSource><<<static_cast<unsigned>(blocks), 256, 0, stream>>>(
-      RecordSource{records}, count, tracks, stride, slot, counters, diagnostics);
+      RecordSource{records}, count, tracks, stride, slot, counters, diagnostics, terms);
   return cudaGetLastError();
 }
 
 cudaError_t launch_ingest_columns(c8r_track_columns const& columns, uint64_t count, double* tracks,
                                   uint64_t stride, unsigned long long* slot, DeviceCounters* counters,
-                                  bool diagnostics, cudaStream_t stream) {
+                                  bool diagnostics, IngestTerms const& terms, cudaStream_t stream) {
   if (count == 0) return cudaSuccess;
   uint64_t const blocks = (count + 255) / 256;
   ingest_kernel<ColumnSource><<<static_cast<unsigned>(blocks), 256, 0, stream>>>(
-      ColumnSource{columns}, count, tracks, stride, slot, counters, diagnostics);
+      ColumnSource{columns}, count, tracks, stride, slot, counters, diagnostics, terms);
   return cudaGetLastError();
+}
+
+bool shared_destination(ObserverCache const* observers, std::size_t count, Destination& out) {
+  if (count == 0) return false;
+  Destination const first = destination_of_host(observers[0]);
+  for (std::size_t i = 1; i < count; ++i) {
+    Destination const d = destination_of_host(observers[i]);
+    if (std::memcmp(&d.height, &first.height, sizeof(double)) != 0 || d.index != first.index ||
+        std::memcmp(&d.n, &first.n, sizeof(double)) != 0 ||
+        std::memcmp(&d.integral, &first.integral, sizeof(double)) != 0)
+      return false;
+  }
+  out = first;
+  return true;
 }
 
 cudaError_t launch_direct(EventPlan const& event, uint64_t track_bound, bool coreas, bool zhs,
@@ -1579,6 +1803,18 @@ cudaError_t launch_direct(EventPlan const& event, uint64_t track_bound, bool cor
   return precision == Precision::kFP64
              ? direct_dispatch<false, double>(event, track_bound, coreas, zhs, stream)
              : direct_dispatch<false, float>(event, track_bound, coreas, zhs, stream);
+}
+
+cudaError_t launch_tiled(EventPlan const& event, uint64_t track_bound, bool coreas, bool zhs,
+                         bool fixed, Precision precision, cudaStream_t stream) {
+  if (fixed) {
+    return precision == Precision::kFP64
+               ? tiled_dispatch<true, double>(event, track_bound, coreas, zhs, stream)
+               : tiled_dispatch<true, float>(event, track_bound, coreas, zhs, stream);
+  }
+  return precision == Precision::kFP64
+             ? tiled_dispatch<false, double>(event, track_bound, coreas, zhs, stream)
+             : tiled_dispatch<false, float>(event, track_bound, coreas, zhs, stream);
 }
 
 cudaError_t launch_windowed(WorkPlan const& plan, bool fixed, Precision precision, int ctas,

@@ -58,7 +58,23 @@ struct EventPlan {
   uint32_t window;               // shared-memory bins per item (<= kernel window)
   uint64_t first_track;          // chunk c covers first_track + c * chunk_size onwards,
   uint64_t last_track;           // clipped to [.., last_track) and the valid tracks
+  uint32_t precomputed;          // tracks carry their source terms (every observer shares
+                                 // one destination row; see IngestTerms)
+  uint32_t pad_;
 };
+
+// Source terms written at ingest: when every observer of an event shares one
+// destination row (always in a homogeneous medium), each track record gets
+// the propagation terms of its start, end and two midpoints for that row,
+// and the windowed kernels read them instead of looking them up per pair.
+struct IngestTerms {
+  int32_t enabled;
+  int32_t pad_;
+  Propagation propagation;
+  Destination destination;
+};
+// The destination row shared by all `count` observers, if they share one.
+bool shared_destination(ObserverCache const* observers, std::size_t count, Destination& out);
 
 // Persistent windowed launch over a work list of (event, chunk, algorithm,
 // observer) items drawn from an atomic counter.  Passed as a __grid_constant__
@@ -78,6 +94,9 @@ struct WorkPlan {
   // (at least the longest chunk of the plan; deferred_list_stride below).
   unsigned int* deferred;
   uint32_t deferred_stride;
+  // Items run again with checked window adds (the unchecked run's bound did
+  // not hold); counted when not null.
+  unsigned long long* reruns;
 };
 
 // Entries per CTA of a launch's deferred lists: the plan's longest chunk.
@@ -137,18 +156,25 @@ enum class Precision : int { kFP64 = 0, kMixed = 1 };
 // valid tracks written.
 cudaError_t launch_ingest(const c8r_lepton_transport_record* records, uint64_t count,
                           double* tracks, uint64_t stride, unsigned long long* slot,
-                          DeviceCounters* counters, bool diagnostics, cudaStream_t stream);
+                          DeviceCounters* counters, bool diagnostics, IngestTerms const& terms,
+                          cudaStream_t stream);
 
 // The same ingest from a structure-of-arrays view of the steps.
 cudaError_t launch_ingest_columns(c8r_track_columns const& columns, uint64_t count, double* tracks,
                                   uint64_t stride, unsigned long long* slot, DeviceCounters* counters,
-                                  bool diagnostics, cudaStream_t stream);
+                                  bool diagnostics, IngestTerms const& terms, cudaStream_t stream);
 
 // Direct pair kernel: one thread per (track, observer) pair, global atomics.
 // The valid-track count is read on the device; `track_bound` (the record
 // count) bounds the grid on the host.
 cudaError_t launch_direct(EventPlan const& event, uint64_t track_bound, bool coreas, bool zhs,
                           bool fixed, Precision precision, cudaStream_t stream);
+
+// The reference's large-batch tile shape: 256-thread CTAs over tiles of 8
+// tracks x 32 observers staged in shared memory, one thread per pair, global
+// atomics (RadioTileProjection, RadioAccumulator.inl:13-85).
+cudaError_t launch_tiled(EventPlan const& event, uint64_t track_bound, bool coreas, bool zhs,
+                         bool fixed, Precision precision, cudaStream_t stream);
 
 // Persistent windowed kernel.  `ctas` persistent CTAs of `threads` threads.
 // The plan needs plan.deferred with ctas * deferred_stride entries and

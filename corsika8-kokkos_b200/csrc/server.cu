@@ -147,6 +147,7 @@ struct ServedEvent {
   double* float_traces[2] = {nullptr, nullptr};
   DeviceCounters* counters = nullptr;
   Propagation propagation{};
+  IngestTerms terms{};       // source terms written at ingest (shared destination row)
   std::deque<Block> blocks;  // in fill order; the front ones retire first
   std::size_t records = 0;
   uint64_t last_round = 0, rounds = 0;
@@ -348,6 +349,14 @@ class Server {
     prop.table_size = p.table_size;
     prop.refinement = config.zhs_subtrack_refinement;
     prop.table = homogeneous ? nullptr : reinterpret_cast<double2*>(memory + table_off);
+    {
+      std::vector<ObserverCache> all(caches[0]);
+      all.insert(all.end(), caches[1].begin(), caches[1].end());
+      Destination d{};
+      ev->terms.enabled = shared_destination(all.data(), all.size(), d) ? 1 : 0;
+      ev->terms.propagation = prop;
+      ev->terms.destination = d;
+    }
     Block b = make_block(block);
     try {
       check(cudaMemsetAsync(memory, 0, bytes, admit_), "server admission");
@@ -403,7 +412,7 @@ class Server {
       }
       std::size_t const n = std::min<std::size_t>(count - done, block_tracks_ - b->records);
       check(launch_ingest(records + done, n, b->tracks, block_tracks_, b->slot, ev.counters,
-                          ev.diagnostics, stream),
+                          ev.diagnostics, ev.terms, stream),
             "server ingest launch");
       check(cudaEventRecord(b->ingested, stream), "server ingest event");
       b->records += n;
@@ -742,6 +751,7 @@ class Server {
           e.first_track = static_cast<uint64_t>(s.chunk_begin) * chunk_tracks_;
           e.last_track = e.first_track + static_cast<uint64_t>(s.chunks) * chunk_tracks_;
           e.window = ev.window;
+          e.precomputed = static_cast<uint32_t>(ev.terms.enabled);
           window = std::max(window, ev.window);
           members.push_back(e);
         }

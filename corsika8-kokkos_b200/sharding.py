@@ -44,17 +44,44 @@ def antenna_shard(observers: np.ndarray, rank: int, world: int) -> tuple:
 
 
 def merge_track_shards(coreas: np.ndarray, zhs: np.ndarray, group=None) -> tuple:
-    """Exact sum over ranks of int64 fixed-point traces (every rank gets it)."""
+    """Exact sum over ranks of int64 fixed-point traces (every rank gets it).
+
+    Each value is split into a signed high and an unsigned low 32-bit half,
+    and the halves are summed over the ranks as int64 (no half sum can leave
+    the int64 range below 2^31 ranks), so the reduction cannot wrap.  The
+    total is then rebuilt and checked: if any bin's exact sum lies outside the
+    int64 range, OverflowError is raised on every rank and nothing is
+    returned, as CooperativeRadioMerge::commit rejects an overflowing merge
+    before writing a bin (CooperativeRadioMerge.inl:180-202,
+    FixedAccumulatorMerge.inl:12-29)."""
     import torch
     import torch.distributed as dist
 
-    out = []
+    halves = []
+    shapes = []
     for traces in (coreas, zhs):
-        t = torch.from_numpy(np.ascontiguousarray(traces, dtype=np.int64)).clone()
-        if _device_backend(group):
-            t = t.cuda()
-        dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
-        out.append(t.cpu().numpy())
+        values = np.ascontiguousarray(traces, dtype=np.int64)
+        shapes.append(values.shape)
+        flat = values.reshape(-1)
+        halves.append(flat >> 32)                   # signed high half
+        halves.append(flat & np.int64(0xFFFFFFFF))  # unsigned low half
+    t = torch.from_numpy(np.concatenate(halves)).clone()
+    if _device_backend(group):
+        t = t.cuda()
+    dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    summed = t.cpu().numpy()
+    out, offset, bad = [], 0, False
+    for shape in shapes:
+        n = int(np.prod(shape))
+        high = summed[offset: offset + n]
+        low = summed[offset + n: offset + 2 * n]
+        offset += 2 * n
+        high = high + (low >> 32)                   # carry of the low sums
+        low = low & np.int64(0xFFFFFFFF)
+        bad = bad or bool(np.any((high < -(1 << 31)) | (high >= (1 << 31))))
+        out.append(((high << 32) | low).reshape(shape))
+    if bad:
+        raise OverflowError("cooperative fixed-point accumulation overflow")
     return tuple(out)
 
 

@@ -111,8 +111,14 @@ enum {
   C8R_KERNEL_AUTO = 0,     /* windowed when the trace window fits, else direct */
   C8R_KERNEL_DIRECT = 1,   /* one thread per (track, antenna) pair, global 64-bit
                               atomics per sample: the reference's launch shape */
-  C8R_KERNEL_WINDOWED = 2  /* CTA owns one antenna's trace in shared memory for a
+  C8R_KERNEL_WINDOWED = 2, /* CTA owns one antenna's trace in shared memory for a
                               chunk of tracks; flushed with checked global atomics */
+  C8R_KERNEL_TILED = 3     /* the reference's large-batch shape (RadioTileProjection,
+                              RadioAccumulator.inl:13-85): 256-thread CTAs over tiles
+                              of 8 tracks x 32 observers staged in shared memory, one
+                              thread per pair, global 64-bit atomics per sample (the
+                              reference itself projects batches below 16384 tracks
+                              with the direct shape) */
 };
 
 /* corsika/kokkos/radio/RadioConfig.hpp:21-53 */
@@ -202,6 +208,9 @@ typedef struct c8r_statistics {
   double coreas_kernel_time_ms; /* windowed CoREAS launches alone (timing on) */
   double zhs_kernel_time_ms;    /* windowed ZHS launches alone (timing on) */
   c8r_counters counters;      /* last downloaded device counters */
+  uint64_t window_reruns;     /* windowed work items projected again with checked adds
+                                 (their unchecked run could not exclude an overflow);
+                                 read with the counters at download */
 } c8r_statistics;
 
 /* Measured device rates used as roofline denominators (c8r_probe_peaks). */
@@ -356,6 +365,66 @@ int c8r_download_fields_device(c8r_accumulator* handle, double* coreas_field_xyz
  * bin checked first; C8R_OVERFLOW_ERROR (nothing written) on overflow. */
 int c8r_merge_fixed(long long* destination, const long long* source, size_t count);
 
+/* ---- Cooperative fixed-point export ------------------------------------------
+ * corsika/kokkos/scheduling/CooperativeEndpoint.hpp: the two endpoints that
+ * may each project part of one shower. */
+enum {
+  C8R_ENDPOINT_CUDA = 0,
+  C8R_ENDPOINT_OPENMP = 1
+};
+/* FixedRadioSnapshot (corsika/kokkos/radio/FixedRadioSnapshot.hpp:18-24) as a
+ * view over caller-owned arrays: the final int64 traces of one endpoint of one
+ * shower (ZHS as potential), in the accumulator's SoA order.  Each trace array
+ * holds 3 x the bins of EVERY observer the config lists for its algorithm
+ * (c8r_snapshot_bins), zero for a disabled algorithm. */
+typedef struct c8r_fixed_snapshot {
+  const char* shower_identity;  /* NUL-terminated, non-empty */
+  uint32_t endpoint;            /* C8R_ENDPOINT_* */
+  uint32_t reserved_;
+  const c8r_config* config;     /* the config the endpoint was created with */
+  const long long* coreas;
+  size_t coreas_count;          /* 3 x CoREAS bins */
+  const long long* zhs;
+  size_t zhs_count;             /* 3 x ZHS bins */
+  c8r_counters counters;
+} c8r_fixed_snapshot;
+/* RadioAccumulator::downloadFixed(shower_identity, endpoint)
+ * (RadioAccumulator.inl:359-405): flushes the pending host batch, checks the
+ * identity and endpoint (C8R_INVALID_ARGUMENT, nothing sealed), seals the
+ * accumulator, copies the int64 traces and counters, then validates them
+ * (validate_fixed_radio: an overflowed accumulator gives C8R_INVALID_ARGUMENT
+ * and stays sealed).  C8R_LOGIC_ERROR when disabled, not deterministic,
+ * already downloaded or sealed.  Buffers sized by c8r_snapshot_bins. */
+int c8r_download_fixed_snapshot(c8r_accumulator* handle, const char* shower_identity, uint32_t endpoint,
+                                long long* coreas_xyz, long long* zhs_xyz, c8r_counters* counters);
+/* Bins of every configured observer of each algorithm (snapshot extents / 3). */
+int c8r_snapshot_bins(const c8r_accumulator* handle, size_t* coreas_bins, size_t* zhs_bins);
+/* validate_fixed_radio (CooperativeRadioMerge.inl:142-152). */
+int c8r_validate_fixed_snapshot(const c8r_fixed_snapshot* snapshot);
+/* merge_radio_counters (CooperativeRadioMerge.inl:154-208): destination +=
+ * source; C8R_OVERFLOW_ERROR (destination unchanged) when an integer counter
+ * would wrap or a diagnostic sum or maximum is not finite. */
+int c8r_merge_counters(c8r_counters* destination, const c8r_counters* source);
+/* Message of the last failing snapshot call of this thread without a merge. */
+const char* c8r_snapshot_last_error(void);
+/* CooperativeRadioMerge (CooperativeRadioMerge.hpp:53-65, .inl:240-277): one
+ * shower's identity and config (deep-copied at creation).  commit accepts each
+ * endpoint's snapshot once; it rejects an invalid snapshot, a second commit of
+ * an endpoint, another identity or a config of different physics
+ * (C8R_INVALID_ARGUMENT), an int64 bin or counter overflow of the sum
+ * (C8R_OVERFLOW_ERROR) and any commit after take (C8R_LOGIC_ERROR); a rejected
+ * commit changes nothing.  take writes the merged traces (sized like a
+ * snapshot of the config), counters and the first commit's endpoint once both
+ * endpoints are in; otherwise, or a second time, C8R_LOGIC_ERROR. */
+typedef struct c8r_cooperative_merge c8r_cooperative_merge;
+int c8r_cooperative_merge_create(const char* shower_identity, const c8r_config* config,
+                                 c8r_cooperative_merge** merge);
+void c8r_cooperative_merge_destroy(c8r_cooperative_merge* merge);
+const char* c8r_cooperative_merge_last_error(const c8r_cooperative_merge* merge);
+int c8r_cooperative_merge_commit(c8r_cooperative_merge* merge, const c8r_fixed_snapshot* snapshot);
+int c8r_cooperative_merge_take(c8r_cooperative_merge* merge, long long* coreas_xyz, long long* zhs_xyz,
+                               c8r_counters* counters, uint32_t* endpoint);
+
 /* ---- Track spool, version 1: completed host tracks on disk ----------------
  * corsika/kokkos/radio/RadioTrackSpoolFormat.hpp:24-29 and
  * RadioTrackSpool{Reader,Writer}.hpp: a 32-byte header ("C8_RADIO_TRACKS\0",
@@ -465,11 +534,17 @@ int c8r_server_get_stats(const c8r_server* server, c8r_server_stats* stats);
  * accumulator's trace layout and units: rows [X | Y | Z] of the algorithm's
  * total bins, observers in config order; long long fixed-point values when
  * config->deterministic (as c8r_download_fixed returns them), else double.
- * `counters` is a device c8r_counters added into, or NULL.  The caller zeroes
- * traces and counters before its first call; later calls add to them, as
- * c8r_accumulate_device does.  config->kernel is ignored (always the windowed
- * projection).  Host arrays of the config are read before the call returns;
- * the work itself is queued on `stream`.
+ * `counters` is a device c8r_counters added into, or NULL.  Fixed-point
+ * overflows are reported only through counters->fixed_point_overflows (the
+ * call itself does not wait for the GPU): a caller that passes NULL gives up
+ * overflow detection.  The caller zeroes traces and counters before its
+ * first call; later calls add to them, as c8r_accumulate_device does.
+ * config->kernel is ignored (always the windowed projection).  Every host
+ * array of the config (observers, refractivity tables) has been read when
+ * the call returns: observer constants and the table travel to the device as
+ * kernel parameters, so the call does not wait for earlier work on `stream`
+ * whatever memory those arrays are in.  The work itself is queued on
+ * `stream`.  A call with count == 0 does nothing on the device.
  *
  * Scratch: one static device array of C8R_NO_ALLOC_SCRATCH_BYTES per GPU that
  * loads this library's module, held until the process exits.  The call calls

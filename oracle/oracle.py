@@ -22,16 +22,19 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 RESTATEMENT = HERE / "liboracle.so"
 REFERENCE = HERE / "_ref" / "libc8ref.so"
-REFERENCE_TREE = Path(os.environ.get("C8R_REFERENCE_TREE", "/root/reference"))
 
 
-def build(reference: bool = True) -> None:
-    """Builds liboracle.so and, where the reference tree exists, _ref/libc8ref.so."""
+def build(reference_tree: str | os.PathLike | None = None) -> None:
+    """Builds liboracle.so and, when a reference source tree is named (the
+    argument, else the C8R_REFERENCE_TREE environment variable) and exists,
+    _ref/libc8ref.so from that tree's unmodified projection sources."""
+    tree = reference_tree or os.environ.get("C8R_REFERENCE_TREE")
     targets = ["oracle"]
-    if reference and (REFERENCE_TREE / "corsika").is_dir():
+    extra = []
+    if tree and (Path(tree) / "corsika").is_dir():
         targets.append("ref")
-    subprocess.run(["make", "-s", "-C", str(HERE), *targets,
-                    f"REFERENCE={REFERENCE_TREE}"], check=True)
+        extra.append(f"REFERENCE={tree}")
+    subprocess.run(["make", "-s", "-C", str(HERE), *targets, *extra], check=True)
 
 
 class _Backend:

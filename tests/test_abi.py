@@ -40,7 +40,8 @@ int main(void) {
   S(c8r_particle_state) S(c8r_lepton_transport_record) S(c8r_observer_snapshot)
   S(c8r_propagation_snapshot) S(c8r_config) S(c8r_tuning) S(c8r_counters) S(c8r_statistics)
   S(c8r_server_options) S(c8r_server_event_info) S(c8r_server_stats)
-  S(c8r_track_segment) S(c8r_track_columns)
+  S(c8r_track_segment) S(c8r_track_columns) S(c8r_fixed_snapshot)
+  O(c8r_fixed_snapshot, config) O(c8r_fixed_snapshot, counters)
   O(c8r_lepton_transport_record, start) O(c8r_lepton_transport_record, end)
   O(c8r_config, propagation) O(c8r_config, precision) O(c8r_config, count_samples)
   return 0;
@@ -73,6 +74,9 @@ def test_struct_layouts_match_the_c_compiler(pkg, tmp_path):
     assert c["c8r_server_stats"] == C.sizeof(abi.ServerStats)
     assert c["c8r_track_segment"] == abi.TRACK_SEGMENT.itemsize
     assert c["c8r_track_columns"] == C.sizeof(abi.TrackColumns)
+    assert c["c8r_fixed_snapshot"] == C.sizeof(abi.FixedSnapshot)
+    assert c["c8r_fixed_snapshot.config"] == abi.FixedSnapshot.config.offset
+    assert c["c8r_fixed_snapshot.counters"] == abi.FixedSnapshot.counters.offset
 
 
 def test_validation_and_memory_projection_on_the_host(pkg, showers):

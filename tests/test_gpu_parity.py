@@ -11,7 +11,7 @@ import cases
 
 pytestmark = pytest.mark.gpu
 
-KERNELS = {"direct": 1, "windowed": 2}
+KERNELS = {"direct": 1, "windowed": 2, "tiled": 3}
 EXACT_COUNTERS = ("coreas_contributions", "zhs_contributions", "zhs_subtracks", "valid_tracks",
                   "fixed_point_overflows")
 
@@ -352,10 +352,68 @@ def test_window_rerun_near_the_fixed_point_limit(pkg, oracle, showers, torch_cud
                         tuning=pkg.TuningParameters(track_tile_size=256))
     assert np.array_equal(got[0], small[0]) and np.array_equal(got[1], small[1])
     assert got[2]["fixed_point_overflows"] == 0
+    assert got[3].window_reruns >= 1  # the bound tripped: an item ran again with checked adds
     assert max(np.abs(got[0]).max(), np.abs(got[1]).max()) > 2 ** 61
     if precision == 0:
         want = oracle.restatement().project(config, records, threads=8)
         assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
+
+
+def heavy_zhs_records(pkg, count, seed):
+    """Slow e- (beta 0.1) moving away from an antenna at the origin, 1 km below,
+    3 deg off the line of sight: each track is one undivided ZHS segment
+    (Fraunhofer number ~0.3) whose detection times span about 8000 bins at
+    10 GHz.  Returns (records, trace start time)."""
+    from corsika8_kokkos_b200 import showers
+
+    rng = np.random.default_rng(seed)
+    c = showers.SPEED_OF_LIGHT
+    beta, duration = 0.1, 727e-9
+    tilt = np.radians(3.0)
+    direction = np.array([np.sin(tilt), 0.0, np.cos(tilt)])
+    start = np.zeros((count, 3))
+    start[:, 0] = rng.uniform(-1.0, 1.0, count)
+    start[:, 1] = rng.uniform(-1.0, 1.0, count)
+    start[:, 2] = 1000.0
+    t_start = rng.uniform(0.0, 1e-9, count)
+    seg = dict(start=start, end=start + beta * c * duration * direction, t_start=t_start,
+               t_end=t_start + duration, pid=np.full(count, 11, np.int32), energy_gev=np.full(count, 5.14e-4),
+               direction=np.tile(direction, (count, 1)), weight=np.ones(count))
+    # detection time of the first sample: midpoint travel time less n beta.k (t_mid - t_start)
+    mid = 1000.0 + 0.5 * beta * c * duration * np.cos(tilt)
+    first = mid / c - beta * np.cos(tilt) * 0.5 * duration
+    return showers.to_records(seg), first - 5e-9
+
+
+def test_window_cap_on_adds_per_thread(pkg, oracle, showers, torch_cuda):
+    """The unchecked window adds rely on an FP32 sum of |increments| per
+    thread, valid while a thread makes fewer than 2^22 adds in an item.  One
+    item of 240000 heavy ZHS tracks (about 8000 samples each: 1.9e9 samples,
+    about 5e6 a thread of a 384-thread CTA) passes the cap and must be
+    projected again with checked adds; one of 100000 tracks (about 2e6 a
+    thread) stays below it and must not.  Both equal the oracle bit for bit."""
+    from corsika8_kokkos_b200 import FlatAtmosphereSnapshot, RadioConfig
+
+    for count, over in ((240_000, True), (100_000, False)):
+        records, start = heavy_zhs_records(pkg, count, seed=count)
+        observer = np.zeros(1, pkg.abi.OBSERVER)
+        observer[0]["start_time_s"] = start
+        observer[0]["duration_s"] = 8191 / 1e10
+        observer[0]["sample_rate_hz"] = 1e10
+        observer[0]["number_of_bins"] = 8192
+        config = RadioConfig(enabled=True, coreas_enabled=False, zhs_enabled=True, deterministic=True,
+                             propagation=FlatAtmosphereSnapshot(homogeneous_refractive_index=1.0),
+                             coreas_observers=np.zeros(0, pkg.abi.OBSERVER), zhs_observers=observer,
+                             precision=0, kernel=2)
+        # work items of 1M tracks: the plan ends on quarter-length items
+        # (262144 tracks), so each case is one item holding every track
+        got = gpu_project(pkg, torch_cuda, config, records,
+                          tuning=pkg.TuningParameters(team_size=384, track_tile_size=1 << 20))
+        want = oracle.restatement().project(config, records, threads=16)
+        assert_same(got[:3], want, True)
+        per_thread = want[2]["zhs_contributions"] / 384
+        assert (per_thread > 2 ** 22) == over, per_thread
+        assert (got[3].window_reruns >= 1) == over, got[3].window_reruns
 
 
 @pytest.mark.parametrize("precision", [0, 1])

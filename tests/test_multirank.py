@@ -1,6 +1,7 @@
 """Two ranks over gloo on CPU: the sharding of one shower's projection
 (track shards merged by an exact int64 sum, antenna shards gathered) gives the
-traces of the unsharded projection bit for bit, and the benchmark's
+traces of the unsharded projection bit for bit, an overflowing track-shard
+merge is reported on every rank instead of wrapping, and the benchmark's
 max-over-ranks reduction.  The projection itself is the oracle here (no GPU);
 the host logic under test is the one bench.py and a multi-GPU caller use."""
 import os
@@ -50,6 +51,23 @@ def _worker(rank, world, port):
         assert np.array_equal(gathered, full[0])
         gathered = sharding.gather_antenna_shards(local[1], observers)
         assert np.array_equal(gathered, full[1])
+
+        # values near the int64 limits: exact where the total fits, an error on
+        # every rank where it does not (the ranks' sum is never wrapped)
+        sign = 1 if rank == 0 else -1
+        big = sign * np.array([[(1 << 63) - 1, -(1 << 63) + 1, -1]], dtype=np.int64)
+        merged = sharding.merge_track_shards(big, -big)
+        assert not merged[0].any() and not merged[1].any()
+        near = np.full((1, 4), (1 << 62) - 1 + rank, dtype=np.int64)
+        summed = sharding.merge_track_shards(near, -near)
+        assert np.array_equal(summed[0], np.full((1, 4), (1 << 63) - 1, dtype=np.int64))
+        try:
+            sharding.merge_track_shards(np.full((1, 2), 1 << 62, dtype=np.int64),
+                                        np.zeros((1, 2), dtype=np.int64))
+        except OverflowError:
+            pass
+        else:
+            raise AssertionError("an overflowing merge was not reported")
 
         assert sharding.max_over_ranks(float(rank + 1)) == float(world)
     finally:
