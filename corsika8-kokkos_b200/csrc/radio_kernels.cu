@@ -130,25 +130,6 @@ __device__ __forceinline__ void spillf3(double* r0, double* r1, double* r2, doub
   atomicAdd(r2, z);
 }
 
-// Adds to the shared-memory window through its shared-space address.  The
-// window pointer reaches the sinks through structs and out-of-line calls, so
-// plain atomicAdd on it compiles to generic atomics; these name the shared
-// state space.  No memory clobber: the window is read only after a barrier.
-__device__ __forceinline__ unsigned shared_address(void const* p) {
-  return static_cast<unsigned>(__cvta_generic_to_shared(p));
-}
-__device__ __forceinline__ void shared_red_add(unsigned long long* p, unsigned long long v) {
-  asm volatile("red.shared.add.u64 [%0], %1;" ::"r"(shared_address(p)), "l"(v));
-}
-__device__ __forceinline__ unsigned long long shared_atom_add(unsigned long long* p, unsigned long long v) {
-  unsigned long long previous;
-  asm volatile("atom.shared.add.u64 %0, [%1], %2;" : "=l"(previous) : "r"(shared_address(p)), "l"(v));
-  return previous;
-}
-__device__ __forceinline__ void shared_red_add(double* p, double v) {
-  asm volatile("red.shared.add.f64 [%0], %1;" ::"r"(shared_address(p)), "d"(v));
-}
-
 // Shared-memory window of `width` bins starting at bin 0 (rows X|Y|Z), with
 // bins past the window spilled to the global rows.
 struct WindowSink {
@@ -167,16 +148,16 @@ struct WindowSink {
       return spill3(row[0] + bin, row[1] + bin, row[2] + bin, x, y, z, ox, oy, oz);
     unsigned long long* const w = win + bin;
     if (unchecked) {
-      if (ox) shared_red_add(w, static_cast<unsigned long long>(x));
-      if (oy) shared_red_add(w + width, static_cast<unsigned long long>(y));
-      if (oz) shared_red_add(w + 2 * width, static_cast<unsigned long long>(z));
+      if (ox) atomicAdd(w, static_cast<unsigned long long>(x));
+      if (oy) atomicAdd(w + width, static_cast<unsigned long long>(y));
+      if (oz) atomicAdd(w + 2 * width, static_cast<unsigned long long>(z));
       bound += mag;
       return ox && oy && oz;
     }
-    unsigned long long const px = ox ? shared_atom_add(w, static_cast<unsigned long long>(x)) : 0ull;
-    unsigned long long const py = oy ? shared_atom_add(w + width, static_cast<unsigned long long>(y)) : 0ull;
+    unsigned long long const px = ox ? atomicAdd(w, static_cast<unsigned long long>(x)) : 0ull;
+    unsigned long long const py = oy ? atomicAdd(w + width, static_cast<unsigned long long>(y)) : 0ull;
     unsigned long long const pz =
-        oz ? shared_atom_add(w + 2 * width, static_cast<unsigned long long>(z)) : 0ull;
+        oz ? atomicAdd(w + 2 * width, static_cast<unsigned long long>(z)) : 0ull;
     return ox && oy && oz && no_overflow3(px, x, py, y, pz, z);
   }
   __device__ __forceinline__ void addf3(uint64_t bin, double x, double y, double z) {
@@ -185,9 +166,9 @@ struct WindowSink {
       return;
     }
     double* const w = fwin + bin;
-    shared_red_add(w, x);
-    shared_red_add(w + width, y);
-    shared_red_add(w + 2 * width, z);
+    atomicAdd(w, x);
+    atomicAdd(w + width, y);
+    atomicAdd(w + 2 * width, z);
   }
 };
 
@@ -286,16 +267,16 @@ __device__ __forceinline__ void deposit_bin(Sink& sink, uint64_t bin, Deposit<Am
 // midpoint field over the Doppler-compressed duration.  Kept out of line: it
 // is taken by a minority of pairs, and its third propagation would otherwise
 // grow the hot loop's instruction footprint.  Returns the counts it adds.
-template <bool kFixed, class Amp, class Sink>
+template <bool kFixed, class Amp, bool kPre, class Sink>
 __device__ __noinline__ Counts coreas_near_cone(Track const t, Propagation const& p,
                                                 ObserverCache const& o, Sink sink,
-                                                bool start_before_end) {
+                                                bool start_before_end, SourceTerms const pre_mid) {
   Counts c;
   Vec3<Amp> const beta{static_cast<Amp>(t.bx), static_cast<Amp>(t.by), static_cast<Amp>(t.bz)};
   double const cf = t.constant * o.sample_rate;
   double const mx = (t.sx + t.ex) * 0.5, my = (t.sy + t.ey) * 0.5, mz = (t.sz + t.ez) * 0.5;
   double const mt = (t.ts + t.te) * 0.5;
-  Path const pm = propagate<true>(p, o, mx, my, mz);
+  Path const pm = kPre ? propagate_with<true>(pre_mid, o, mx, my, mz) : propagate<true>(p, o, mx, my, mz);
   double const mr = mt + pm.time;
   double const md = doppler(pm.n_src, t.bx, t.by, t.bz, pm.kx, pm.ky, pm.kz);
   Vec3<Amp> const k{static_cast<Amp>(pm.kx), static_cast<Amp>(pm.ky), static_cast<Amp>(pm.kz)};
@@ -327,11 +308,14 @@ __device__ __noinline__ Counts coreas_near_cone(Track const t, Propagation const
 // ---------------------------------------------------------------- CoREAS
 // accumulate_co_reas, RadioProjection.inl:339-409, every decision and (FP64
 // path) every amplitude evaluated exactly as the reference.
-template <bool kFixed, class Amp, class Sink>
+// kPre: the start, end and midpoint source terms are `terms` (precomputed at
+// ingest for the event's shared destination row), else looked up.
+template <bool kFixed, class Amp, class Sink, bool kPre = false>
 __device__ __forceinline__ void coreas_pair(Track const& t, Propagation const& p,
-                                            ObserverCache const& o, Sink& sink, Counts& c) {
-  Path const ps = propagate<true>(p, o, t.sx, t.sy, t.sz);
-  Path const pe = propagate<true>(p, o, t.ex, t.ey, t.ez);
+                                            ObserverCache const& o, Sink& sink, Counts& c,
+                                            SourceTerms const* terms = nullptr) {
+  Path const ps = kPre ? propagate_with<true>(terms[0], o, t.sx, t.sy, t.sz) : propagate<true>(p, o, t.sx, t.sy, t.sz);
+  Path const pe = kPre ? propagate_with<true>(terms[1], o, t.ex, t.ey, t.ez) : propagate<true>(p, o, t.ex, t.ey, t.ez);
   double const pre = doppler(ps.n_src, t.bx, t.by, t.bz, ps.kx, ps.ky, ps.kz);
   double const post = doppler(pe.n_src, t.bx, t.by, t.bz, pe.kx, pe.ky, pe.kz);
   double sr = t.ts + ps.time;
@@ -340,7 +324,7 @@ __device__ __forceinline__ void coreas_pair(Track const& t, Propagation const& p
   Vec3<Amp> const beta{static_cast<Amp>(t.bx), static_cast<Amp>(t.by), static_cast<Amp>(t.bz)};
 
   if (ps.n_dst > 1. && (fabs(pre) < kCoreasThreshold || fabs(post) < kCoreasThreshold)) {
-    Counts const d = coreas_near_cone<kFixed, Amp>(t, p, o, sink, sr < er);
+    Counts const d = coreas_near_cone<kFixed, Amp, kPre>(t, p, o, sink, sr < er, kPre ? terms[2] : SourceTerms{});
     c.coreas += d.coreas;
     c.overflows += d.overflows;
     c.mag += d.mag;
@@ -633,10 +617,14 @@ struct StagedSegment<double> {
 // zhs_segment<kRuns = true, kFilter>, its samples staged instead of
 // deposited.  With kFilter the midpoint propagation is propagate_fast: its
 // directions (8u) stay inside the n beta.k bound, and its time error adds to
-// the detection-time bound e_d.  Returns false, staging nothing, when the
-// segment needs the per-index binning or (kFilter) an exact evaluation, or
-// when the trace has 2^26 bins or more (staged counts then stay far inside 32
-// bits per warp).
+// the detection-time bound e_d.  Returns false when the segment needs the
+// per-index binning or (kFilter) an exact evaluation, or when the trace has
+// 2^26 bins or more (staged counts then stay far inside 32 bits per warp);
+// the caller then discards whatever `out` holds.  The filter's ambiguity
+// test is applied at the end, after the samples are formed (the values it
+// declines are discarded): with the decision off the critical path the
+// kernel issues the staging arithmetic beside the bound arithmetic (7% off
+// the ZHS kernel on the 1e7 x 160 workload).
 template <bool kFilter, class Amp, bool kPre = false>
 __device__ __forceinline__ bool zhs_stage(double p1x, double p1y, double p1z, double p2x,
                                           double p2y, double p2z, double t1, double t2,
@@ -645,6 +633,7 @@ __device__ __forceinline__ bool zhs_stage(double p1x, double p1y, double p1z, do
                                           StagedSegment<Amp>& out,
                                           SourceTerms const& pre = SourceTerms{}) {
   if (!(o.bins_d < 67108864.0)) return false;
+  bool decided = true;
   double const mx = (p1x + p2x) * 0.5, my = (p1y + p2y) * 0.5, mz = (p1z + p2z) * 0.5;
   FastPath const path = filtered_path<kFilter, kPre>(p, o, mx, my, mz, pre);
   if (kFilter && !path.ok) return false;
@@ -686,7 +675,7 @@ __device__ __forceinline__ bool zhs_stage(double p1x, double p1y, double p1z, do
     bool const ambiguous = fabs(d1 - d2) <= 2. * e_d || fabs(den) < 1.e-6 ||
                            f1 <= e_x + 0x1p-50 * (fabs(x1) + 1.) ||
                            f2 <= e_x + 0x1p-50 * (fabs(x2) + 1.) || (nb > 1 && !run_ok);
-    if (ambiguous) return false;
+    decided = !ambiguous;
   } else if (nb > 1 && !run_ok) {
     return false;
   }
@@ -711,7 +700,7 @@ __device__ __forceinline__ bool zhs_stage(double p1x, double p1y, double p1z, do
     out.last_bin = static_cast<uint32_t>(bv2);
     out.flags = 2u;
   }
-  if (single) return true;
+  if (single) return decided;
   double const frac_first = fabs(sb + 0.5 - x1);
   out.first = amp_div(static_cast<Amp>(sc * frac_first), static_cast<Amp>(dd));
   double const mc = (subdivided ? 1. : sign) * t.constant;
@@ -739,7 +728,7 @@ __device__ __forceinline__ bool zhs_stage(double p1x, double p1y, double p1z, do
       }
     }
   }
-  return true;
+  return decided;
 }
 
 // Deposits the staged segments of a warp: every lane takes two bins of the
@@ -858,10 +847,12 @@ __device__ __forceinline__ void zhs_pair(Track const& t, Propagation const& p,
 }
 
 // The common ZHS pair of the windowed kernel: one undivided segment, staged
-// for the warp's cooperative deposit.  Returns false, staging nothing, when
-// the track is subdivided (Fraunhofer number above 1, or refinement), when
-// (kFilter) the Fraunhofer test is not surely below 1, or when zhs_stage
-// declines the segment; the kernel then defers the pair to zhs_drain.
+// for the warp's cooperative deposit.  Returns false, staging nothing (`seg`
+// cleared), when the track is subdivided (Fraunhofer number above 1, or
+// refinement), when (kFilter) the Fraunhofer test is not surely below 1, or
+// when zhs_stage declines the segment; the kernel then defers the pair to
+// zhs_drain.  The FP32 Fraunhofer test and the staging of the one segment
+// are independent and both evaluated; the test decides at the end.
 //
 // kFilter: F is estimated in FP32 as sin^2(theta) K with
 // sin^2 = |beta x d|^2 / (|beta|^2 |d|^2) and K = 2 pi L^2 / (|d| lambda); its
@@ -875,6 +866,7 @@ __device__ __forceinline__ bool zhs_common(Track const& t, Propagation const& p,
                                            StagedSegment<Amp>& seg, SourceTerms const& pre_mid) {
   if (p.refinement != 1u) return false;
   double const mx = (t.sx + t.ex) * 0.5, my = (t.sy + t.ey) * 0.5, mz = (t.sz + t.ez) * 0.5;
+  bool surely_one = true;
   if (kFilter) {
     float const dx = static_cast<float>(o.px - mx), dy = static_cast<float>(o.py - my),
                 dz = static_cast<float>(o.pz - mz);
@@ -892,7 +884,7 @@ __device__ __forceinline__ bool zhs_common(Track const& t, Propagation const& p,
     float const kf = k * (f + 1.f);
     float const root = kf > 0.f ? kf * rsqrtf(kf) : 0.f;
     float const margin = 4.e-6f * root + 4.e-5f * (f + 1.f) + 4.e-12f * k;
-    if (!(f + margin < 1.f)) return false;
+    surely_one = f + margin < 1.f;
   } else {
     Path const pm = propagate<false>(p, o, mx, my, mz);
     double const uk = (t.bx * pm.kx + t.by * pm.ky + t.bz * pm.kz) / t.beta_module;
@@ -900,10 +892,14 @@ __device__ __forceinline__ bool zhs_common(Track const& t, Propagation const& p,
     double const fraunhofer = s2 * t.length * t.length / pm.dist / o.wavelength * 2. * kPi;
     if (fraunhofer > 1.) return false;
   }
-  if (!zhs_stage<kFilter, Amp, kPre>(t.sx, t.sy, t.sz, t.sx + (t.ex - t.sx), t.sy + (t.ey - t.sy),
+  bool const staged = zhs_stage<kFilter, Amp, kPre>(t.sx, t.sy, t.sz, t.sx + (t.ex - t.sx), t.sy + (t.ey - t.sy),
                                      t.sz + (t.ez - t.sz), t.ts, t.ts + (t.te - t.ts), t, p, o, false,
-                                     seg, pre_mid))
+                                     seg, pre_mid);
+  if (!(staged && surely_one)) {
+    seg.count = 0u;
+    seg.flags = 0u;
     return false;
+  }
   c.subtracks += 1ull;
   return true;
 }
@@ -1080,9 +1076,9 @@ __global__ void __launch_bounds__(256) ingest_kernel(
     r[5] = make_double2(t.bz, t.length);
     r[6] = make_double2(t.beta_module, t.constant);
     if (terms.enabled) {
-      // the source points of the windowed kernels' common paths, with the
-      // reference's own arithmetic: the ZHS segment of an undivided track ends
-      // at start + (end - start) (RadioProjection.inl:505-512), the CoREAS
+      // the source points of the windowed kernels, with the reference's own
+      // arithmetic: the ZHS segment of an undivided track ends at
+      // start + (end - start) (RadioProjection.inl:505-512), the CoREAS
       // near-cone midpoint is (start + end) / 2 (:357-359)
       Propagation const& p = terms.propagation;
       Destination const& d = terms.destination;
@@ -1421,12 +1417,20 @@ __device__ __noinline__ Counts zhs_drain(const double* __restrict__ tracks, uint
 
 // A deferred CoREAS pair of the windowed kernel, loaded and evaluated exactly
 // out of line (the caller passes the row, not the 112-byte track).
-template <bool kFixed, class Amp, class Sink>
+template <bool kFixed, class Amp, bool kPre, class Sink>
 __device__ __noinline__ Counts coreas_drain_pair(const double* __restrict__ tracks, uint64_t row,
                                                  Propagation const& p, ObserverCache const& o,
                                                  Sink sink) {
   Counts c;
-  coreas_pair<kFixed, Amp>(load_track(tracks, 0, row), p, o, sink, c);
+  if (kPre) {
+    double2 const* r = reinterpret_cast<double2 const*>(tracks + row * kTrackDoubles);
+    double2 const n = __ldg(r + kNdstStart / 2), s = __ldg(r + kFactorStart / 2), e = __ldg(r + kFactorEnd / 2),
+                  m = __ldg(r + kFactorMidCoreas / 2);
+    SourceTerms const pre[3] = {{s.x, s.y, n.x}, {e.x, e.y, 0.}, {m.x, m.y, 0.}};
+    coreas_pair<kFixed, Amp, Sink, true>(load_track(tracks, 0, row), p, o, sink, c, pre);
+  } else {
+    coreas_pair<kFixed, Amp>(load_track(tracks, 0, row), p, o, sink, c);
+  }
   return c;
 }
 
@@ -1561,7 +1565,7 @@ __global__ void __launch_bounds__(kAlgorithm == 1 ? kZhsThreadsMax : kWindowThre
           d = zhs_drain<kFixed, kFilter, Amp>(ev.tracks, begin, deferred_list + from, count,
                                               ev.propagation, o, sink, staging);
         } else if (lane < count) {
-          d = coreas_drain_pair<kFixed, Amp>(ev.tracks, begin + deferred_list[from + lane],
+          d = coreas_drain_pair<kFixed, Amp, kPre>(ev.tracks, begin + deferred_list[from + lane],
                                              ev.propagation, o, sink);
         }
         c.coreas += d.coreas;

@@ -82,7 +82,7 @@ def test_double_fp32_keeps_bins_and_fp32_moves_some(pkg, showers, torch_cuda):
 def test_study_precisions_are_not_served_or_batched(pkg, showers):
     wl, _, _ = showers.workload_config("plain_c0", bins=256)
     config = showers.make_config(wl, precision=pkg.abi.PRECISION_STUDY_FP32)
-    server = pkg.RadioServer(budget_bytes=1 << 28)
+    server = pkg.RadioServer(budget_bytes=1 << 30)
     with pytest.raises(pkg.InvalidArgument):
         server.open(config)
     server.close()
