@@ -43,7 +43,9 @@ FLOP_COREAS_PAIR = 108 + 14   # two propagations, two Doppler factors, two field
 FLOP_ZHS_SETUP = 40 + 12      # Fraunhofer midpoint propagation and subdivision
 FLOP_ZHS_SUBTRACK = 79 + 7    # one segment: propagation, detection times, potential
 FLOP_SAMPLE = 12 + 3          # bin, gate and three fixed-point conversions
-TRACK_BYTES = 128             # algorithmic read per track per launch (packed kinematics)
+TRACK_RECORD_BYTES = 192      # kinematics record per track (with the precomputed source terms)
+# algorithmic read per track per launch: the record fields each kernel's common path loads
+TRACK_BYTES = {"coreas": 160, "zhs": 128}
 L2_BYTES = 126 << 20          # B200 L2
 
 WORKLOAD_NAME = "tiled_c1"
@@ -77,6 +79,9 @@ def parse_args():
     p.add_argument("--batched", action="store_true",
                    help="print the batched workload (64 events, one graph-replayed launch per algorithm) instead")
     p.add_argument("--batch-events", type=int, default=64)
+    p.add_argument("--no-batched", action="store_true", help="skip the batched leg of the default run")
+    p.add_argument("--tuning-cache", default=str(Path(tempfile.gettempdir()) / "c8radio-b200.tuning"),
+                   help="tuning cache file the batched leg reads and, after autotuning, writes")
     p.add_argument("--precision-study", action="store_true",
                    help="print the arrival-time precision study of the ice workload instead")
     p.add_argument("--plain-fraction", type=int, default=8,
@@ -241,7 +246,7 @@ def run_ours(args):
 
     # inputs smaller than twice the 126 MB L2: each step is timed alone, with a
     # 512 MB buffer written between steps (outside the timed windows)
-    input_bytes = records.nbytes + n * TRACK_BYTES
+    input_bytes = records.nbytes + n * TRACK_RECORD_BYTES
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda") if input_bytes < 2 * L2_BYTES else None
 
     def timed_run(precision, kernel, steps, warmup, timing=True):
@@ -347,11 +352,11 @@ def run_ours(args):
         return {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": achieved / peak if achieved and peak else None,
                 "traffic": traffic.get(key), "kernel_ms": ms, "flop_per_launch": flops,
-                "bytes_per_launch_algorithmic": TRACK_BYTES * n}
+                "bytes_per_launch_algorithmic": TRACK_BYTES[key] * n}
 
     roofline = roof(zhs_flops, zhs_ms, "zhs")
     roofline.update({
-        "kernel": "windowed_kernel<fixed,float,ZHS> (dominant, 2/3 of the step)",
+        "kernel": "windowed_kernel<fixed,float,ZHS> (dominant, 62% of the step)",
         "peak_source": "FP64 FMA stream measured in this run on this GPU (c8r_probe_peaks); "
                        "of measured",
         "traffic_source": ("DRAM bytes read + written per track from an ncu capture of the same "
@@ -375,11 +380,18 @@ def run_ours(args):
 
     # the served stream runs before the CPU baseline: its latencies depend on the
     # host threads that feed it, which the baseline's worker threads would crowd
-    serving = None
-    if rank == 0 and world == 1 and not args.no_serving:
+    serving = batched = None
+    if rank == 0 and world == 1 and not (args.no_serving and args.no_batched):
         del device_records
         torch.cuda.empty_cache()
-        serving = run_serving(pkg, showers, torch, args, local)
+        library = showers.shower_library(args.library_segments)
+        dev = {k: torch.from_numpy(v.view(np.uint8).reshape(-1)).cuda() for k, v in library.items()}
+        if not args.no_serving:
+            serving = run_serving(pkg, showers, torch, args, local, library, dev)
+        if not args.no_batched:
+            batched = batched_leg(pkg, showers, torch, args, library, dev, steps=3, warmup=1)
+        del dev
+        torch.cuda.empty_cache()
 
     baseline = None
     if rank == 0 and world == 1 and not args.no_baseline:
@@ -405,7 +417,7 @@ def run_ours(args):
                    "algorithms": "CoREAS+ZHS fused", "precision": args.precision,
                    "kernel": args.kernel, "pairs_per_step": pairs_per_step,
                    "l2": (f"inputs larger than L2 ({records.nbytes / 1e9:.2f} GB records, "
-                          f"{n * TRACK_BYTES / 1e9:.2f} GB kinematics)") if flush is None else
+                          f"{n * TRACK_RECORD_BYTES / 1e9:.2f} GB kinematics)") if flush is None else
                          (f"L2 flushed between steps (512 MB written; inputs "
                           f"{input_bytes / 1e6:.0f} MB), steps timed alone")},
         "e2e": e2e, "roofline": roofline, "cpu_baseline": baseline,
@@ -414,6 +426,7 @@ def run_ours(args):
                                               "zhs_contributions", "zhs_subtracks",
                                               "fixed_point_overflows")},
         "variants": variants, "accuracy": accuracy, "peaks": peaks, "serving": serving,
+        "batched": batched,
     }
     print(json.dumps(line), flush=True)
 
@@ -463,7 +476,7 @@ def trace_accuracy(pkg, showers, wl, device_records, n, precision, kernel, strea
 
 
 # ------------------------------------------------------------------ served stream
-def run_serving(pkg, showers, torch, args, local: int) -> dict:
+def run_serving(pkg, showers, torch, args, local: int, library: dict, dev: dict) -> dict:
     """The served form: a Poisson stream of batched-workload events with a heavy
     tail, each event opened on a RadioServer at its arrival time by its own
     producer thread, its segments added as device records (replayed from a
@@ -479,9 +492,7 @@ def run_serving(pkg, showers, torch, args, local: int) -> dict:
     served traces' error against the oracle on the smallest events."""
     specs, arrivals = showers.served_event_specs(events=args.serve_events, rate_hz=args.serve_rate)
     size = args.library_segments
-    library = showers.shower_library(size)
     itemsize = next(iter(library.values())).itemsize
-    dev = {k: torch.from_numpy(v.view(np.uint8).reshape(-1)).cuda() for k, v in library.items()}
     configs = [showers.make_config(showers.event_workload(spec)[0], precision=1, kernel=2)
                for spec in specs]
     torch.cuda.synchronize()
@@ -494,24 +505,29 @@ def run_serving(pkg, showers, torch, args, local: int) -> dict:
     stable, _ = serve_stream(pkg, showers, torch, args, local, specs, arrivals * (args.serve_rate / stable_rate),
                              configs, dev, itemsize, size, keep=())
 
-    # plain FP64 drop-in, event by event, on a fixed fraction of each event
-    plain_pairs, plain_seconds = 0, 0.0
+    # plain FP64 drop-in, event by event, on a fixed fraction of each event, in
+    # both of the reference's launch shapes; the comparison takes the faster
     stream = torch.cuda.current_stream()
-    for k, spec in enumerate(specs):
-        count = max(1, spec.segments // args.plain_fraction)
-        wl, _ = showers.event_workload(spec)
-        acc = pkg.RadioAccumulator(showers.make_config(wl, precision=0, kernel=1),
-                                   stream=stream.cuda_stream)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        base = dev[showers.library_key(spec)].data_ptr()
-        for offset, n in showers.replay_slices(count, size):
-            acc.accumulate_lepton_tracks(base + offset * itemsize, n)
-        acc.download_fixed()
-        plain_seconds += time.perf_counter() - t0
-        plain_pairs += count * spec.antennas
-        acc.close()
-    plain = plain_pairs / plain_seconds
+    plain_rates = {}
+    for shape, kernel in (("direct", 1), ("tiled", 3)):
+        plain_pairs, plain_seconds = 0, 0.0
+        for k, spec in enumerate(specs):
+            count = max(1, spec.segments // args.plain_fraction)
+            wl, _ = showers.event_workload(spec)
+            acc = pkg.RadioAccumulator(showers.make_config(wl, precision=0, kernel=kernel),
+                                       stream=stream.cuda_stream)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            base = dev[showers.library_key(spec)].data_ptr()
+            for offset, n in showers.replay_slices(count, size):
+                acc.accumulate_lepton_tracks(base + offset * itemsize, n)
+            acc.download_fixed()
+            plain_seconds += time.perf_counter() - t0
+            plain_pairs += count * spec.antennas
+            acc.close()
+        plain_rates[shape] = plain_pairs / plain_seconds
+    plain_shape = max(plain_rates, key=plain_rates.get)
+    plain = plain_rates[plain_shape]
 
     # served (mixed precision) traces against the oracle -- the reference's FP64
     # arithmetic on the host, as the checker -- per antenna trace, on the
@@ -531,8 +547,6 @@ def run_serving(pkg, showers, torch, args, local: int) -> dict:
             if l2.size:
                 worst = max(worst, float(l2.max()))
                 worst_peak = max(worst_peak, float(peak.max()))
-    del dev
-    torch.cuda.empty_cache()
     tail = sum(1 for s in specs if s.segments == max(x.segments for x in specs))
     stable["rate_hz"] = stable_rate
     stable["rate_source"] = "0.6 x the first run's sustained pairs/s / mean pairs per event"
@@ -546,9 +560,11 @@ def run_serving(pkg, showers, torch, args, local: int) -> dict:
         "budget_gb": args.serve_budget_gb, "events": len(specs), "pairs": int(sum(pairs)),
         "offered_pairs_per_s": sum(pairs) / max(float(arrivals[-1]), 1e-9),
         "plain_event_by_event": {
-            "pairs_per_s": plain,
+            "pairs_per_s": plain, "shape": plain_shape,
+            "pairs_per_s_by_shape": plain_rates,
             "sample": (f"every event of the stream, first 1/{args.plain_fraction} of its segments, "
-                       f"FP64 direct kernel, one accumulator per event (accumulate + download_fixed)")},
+                       f"FP64, the reference's direct and tiled launch shapes (the faster taken), one "
+                       f"accumulator per event (accumulate + download_fixed)")},
         "served_vs_plain": overloaded["pairs_per_s"] / plain,
         "accuracy_vs_oracle": {"max_rel_l2_per_trace": worst, "max_peak_error": worst_peak,
                                "traces": traces, "events": "the 3 smallest events of the stream",
@@ -633,23 +649,32 @@ def serve_stream(pkg, showers, torch, args, local, specs, arrivals, configs, dev
 
 # ------------------------------------------------------------------ batched
 def run_batched(args):
-    """Batched workload: `batch_events` events (segments log-uniform 1e5-2e7,
-    16-300 antennas, zenith 0-60 deg, Xmax 550-850 g/cm^2, 4096 bins), each
-    staged into its own accumulator (mixed precision) from a device-resident
-    library of seeded showers, then projected together by one persistent launch
-    per algorithm, replayed from a captured CUDA graph.  The tile shape (threads
-    per CTA x tracks per work item) is chosen first by the autotuner on the
-    first eighth of the events.  Timed: K graph replays, CUDA events."""
+    """--batched: the batched workload alone, one JSON line."""
     import torch
 
     pkg = entry.load_package()
     from corsika8_kokkos_b200 import showers
 
+    library = showers.shower_library(args.library_segments)
+    dev = {k: torch.from_numpy(v.view(np.uint8).reshape(-1)).cuda() for k, v in library.items()}
+    out = batched_leg(pkg, showers, torch, args, library, dev, steps=args.steps, warmup=args.warmup)
+    print(json.dumps(dict(out, metric="track-antenna pairs/s", unit="pairs/s")), flush=True)
+
+
+def batched_leg(pkg, showers, torch, args, library, dev, steps: int, warmup: int) -> dict:
+    """Batched workload: `batch_events` events (segments log-uniform 1e5-2e7,
+    16-300 antennas, zenith 0-60 deg, Xmax 550-850 g/cm^2, 4096 bins), each
+    staged into its own accumulator (mixed precision) from a device-resident
+    library of seeded showers, then projected together by one persistent launch
+    per algorithm, replayed from a captured CUDA graph.  The tile (track
+    segments per stage = threads per CTA, tracks per work item, bin window; one
+    antenna per CTA) comes from the tuning cache when it holds one for this
+    device, build and workload, else from the autotuner on the first eighth of
+    the events, which is then stored.  Timed: `steps` graph replays, CUDA
+    events."""
     specs = showers.batched_event_specs(events=args.batch_events)
     size = args.library_segments
-    library = showers.shower_library(size)
     itemsize = next(iter(library.values())).itemsize
-    dev = {k: torch.from_numpy(v.view(np.uint8).reshape(-1)).cuda() for k, v in library.items()}
     stream = torch.cuda.Stream()
     events = []
     for spec in specs:
@@ -664,36 +689,51 @@ def run_batched(args):
     stream.synchronize()
     pairs = sum(s.segments * s.antennas for s in specs)
     batch = pkg.RadioBatch(stream=stream.cuda_stream)
-    tune = events[: max(1, len(events) // 8)]
-    best, best_ms = batch.autotune(tune, repetitions=1)
+    label = (f"batched_c3 events={len(specs)} bins=4096 precision=mixed library={size} "
+             f"segments={sum(s.segments for s in specs)}")
+    cache = Path(args.tuning_cache)
+    best = pkg.tuning_cache_load(cache, label)
+    source, tune_ms, tuned_events = "tuning cache", None, 0
+    if best is None:
+        tune = events[: max(1, len(events) // 8)]
+        best, tune_ms = batch.autotune(tune, repetitions=1)
+        pkg.tuning_cache_store(cache, label, best)
+        reloaded = pkg.tuning_cache_load(cache, label, require=True)
+        assert (reloaded.team_size, reloaded.track_tile_size, reloaded.observer_tile_size) == \
+            (best.team_size, best.track_tile_size, best.observer_tile_size)
+        source, tuned_events = "autotuner (stored in the tuning cache)", len(tune)
     for acc in events:
         acc.set_tuning(best)
-    for _ in range(max(1, args.warmup)):
+    for _ in range(max(1, warmup)):
         batch.project(events, graph=True, keep_staged=True)
     stream.synchronize()
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(0) as clocks:
         start.record(stream)
-        for _ in range(args.steps):
+        for _ in range(steps):
             batch.project(events, graph=True, keep_staged=True)
         end.record(stream)
         stream.synchronize()
-    ms = start.elapsed_time(end) / args.steps
+    ms = start.elapsed_time(end) / steps
     captures = batch.graph_captures()
     batch.close()
     for acc in events:
         acc.close()
-    print(json.dumps({
-        "metric": "track-antenna pairs/s", "value": pairs / (ms * 1e-3), "unit": "pairs/s",
+    torch.cuda.empty_cache()
+    return {
+        "value": pairs / (ms * 1e-3),
         "workload": f"batched_c3: {len(specs)} events, segments log-uniform 1e5-2e7, 16-300 antennas, "
                     f"zenith 0-60, Xmax 550-850, 4096 bins, CoREAS+ZHS, mixed precision, fixed point",
         "inputs": f"device-resident replay of 15 seeded library showers ({size} segments each), staged",
         "events": len(specs), "segments": int(sum(s.segments for s in specs)), "pairs_per_step": int(pairs),
-        "steps": args.steps, "ms_per_step": ms, "launches_per_step": 2, "graph_captures": int(captures),
-        "autotune": {"team_size": best.team_size, "track_tile_size": best.track_tile_size,
-                     "ms": best_ms, "events": len(tune)},
+        "steps": steps, "ms_per_step": ms, "launches_per_step": 2, "graph_captures": int(captures),
+        "tile": {"segments_per_stage": best.team_size or 640, "antennas_per_cta": 1,
+                 "bin_window": best.observer_tile_size or 4096,
+                 "tracks_per_item": best.track_tile_size or "auto (about 16 items per CTA)"},
+        "tuning": {"source": source, "autotune_ms_per_projection": tune_ms, "autotune_events": tuned_events,
+                   "workload_label": label},
         "clocks": clocks.summary(),
-    }), flush=True)
+    }
 
 
 # ------------------------------------------------------------------ precision study

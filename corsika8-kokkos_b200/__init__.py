@@ -199,6 +199,28 @@ def probe_peaks() -> dict:
     return {name: getattr(p, name) for name, _ in abi.Peaks._fields_}
 
 
+def tuning_cache_load(path, workload: str, require: bool = False) -> Optional[TuningParameters]:
+    """The tuning stored at `path` for this device, build and workload label,
+    or None when there is none that matches (c8r_tuning_cache_load)."""
+    lib = library()
+    t = abi.Tuning()
+    matched = C.c_int()
+    _raise(lib.c8r_tuning_cache_load(str(path).encode(), workload.encode(), int(require), C.byref(t),
+                                     C.byref(matched)), lib.c8r_tuning_cache_last_error())
+    if not matched.value:
+        return None
+    return TuningParameters(team_size=t.team_size, track_tile_size=t.track_tile_size,
+                            observer_tile_size=t.observer_tile_size)
+
+
+def tuning_cache_store(path, workload: str, tuning: TuningParameters) -> None:
+    """Persists `tuning` for this device, build and workload label (c8r_tuning_cache_store)."""
+    lib = library()
+    t = tuning.to_c()
+    _raise(lib.c8r_tuning_cache_store(str(path).encode(), workload.encode(), C.byref(t)),
+           lib.c8r_tuning_cache_last_error())
+
+
 def validate(config: RadioConfig) -> None:
     lib = library()
     cfg, keep = config.to_c()

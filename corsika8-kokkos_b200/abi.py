@@ -320,6 +320,10 @@ PROTOTYPES = {
     "c8r_batch_autotune": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.c_size_t, C.c_int,
                                      C.POINTER(Tuning), C.POINTER(C.c_double)]),
     "c8r_batch_graph_captures": (C.c_int, [C.c_void_p, C.POINTER(C.c_ulonglong)]),
+    "c8r_tuning_cache_load": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.POINTER(Tuning),
+                                        C.POINTER(C.c_int)]),
+    "c8r_tuning_cache_store": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(Tuning)]),
+    "c8r_tuning_cache_last_error": (C.c_char_p, []),
     "c8r_server_create": (C.c_int, [C.POINTER(ServerOptions), C.POINTER(C.c_void_p)]),
     "c8r_server_destroy": (None, [C.c_void_p]),
     "c8r_server_last_error": (C.c_char_p, [C.c_void_p]),

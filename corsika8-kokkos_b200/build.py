@@ -16,7 +16,7 @@ HERE = Path(__file__).resolve().parent
 CSRC = HERE / "csrc"
 LIBRARY = HERE / "libc8radio.so"
 SOURCES = ["radio_kernels.cu", "accumulator.cu", "probes.cu", "no_alloc.cu", "server.cu",
-           "precision_study.cu", "spool.cu", "snapshot.cu"]
+           "precision_study.cu", "spool.cu", "snapshot.cu", "tuning.cu"]
 HEADERS = ["radio_device.cuh", "radio_kernels.cuh", "host_setup.hpp", "status.hpp"]
 
 NVCC_FLAGS = [

@@ -472,8 +472,14 @@ class Accumulator {
     threads_ = t.team_size ? static_cast<int>(t.team_size) : kWindowThreads;
     tuning_.team_size = t.team_size;
     tuning_.track_tile_size = t.track_tile_size;
+    tuning_.observer_tile_size = t.observer_tile_size;
     stats_.track_tile_size = static_cast<uint32_t>(t.track_tile_size);
+    if (enabled()) {
+      choose_window();
+      stats_.observer_tile_size = static_cast<uint32_t>(window_bins_);
+    }
   }
+  std::size_t largest_bins() const { return largest_bins_; }
   // Zeroes traces and projection counters, keeping staged tracks (autotuning).
   void zero_traces() {
     if (!enabled()) return;
@@ -807,8 +813,15 @@ class Accumulator {
               "decode upload");
       }
     }
+    largest_bins_ = largest;
+    choose_window();
+  }
+
+  // Shared-memory window: the longest trace, capped by the tuning's
+  // observer_tile_size and by what the device's shared memory holds.
+  void choose_window() {
     int const device_window = windowed_max_bins(device_);
-    std::size_t window = largest;
+    std::size_t window = largest_bins_;
     if (tuning_.observer_tile_size != 0) window = std::min<std::size_t>(window, tuning_.observer_tile_size);
     window_bins_ = std::min<std::size_t>(window, static_cast<std::size_t>(device_window));
     if (window_bins_ == 0) window_bins_ = 1;
@@ -1057,6 +1070,7 @@ class Accumulator {
   std::size_t config_bins_[2] = {0, 0};  // all configured observers (snapshot extents)
   uint64_t max_observer_bins_[2] = {0, 0};
   std::size_t window_bins_ = 0;
+  std::size_t largest_bins_ = 0;  // longest trace of the configured observers
   DeviceBuffer<double2> table_;
   DeviceBuffer<ObserverCache> observers_[2];
   DeviceBuffer<unsigned long long> fixed_traces_[2];
@@ -1145,35 +1159,54 @@ class Batch {
     }
   }
 
-  // Sweeps block size x chunk size (tracks per work item) on the staged
-  // events, keeps the fastest, and zeroes the traces it wrote.
+  // Sweeps the tile space of the windowed kernel on the staged events, keeps
+  // the fastest, and zeroes the traces it wrote.  The kernel's tile is one
+  // antenna's window per CTA, a stage of `team_size` track segments (one per
+  // thread) and work items of `track_tile_size` tracks; the sweep takes team
+  // size {256, 384, 512, 640} x tracks per item {auto, 32768, 131072, 524288}
+  // with the whole trace as window, then, at the best pair, bin windows of
+  // {2048, 1024, 512} shorter than the longest trace (bins past a window go
+  // to checked global atomics).
   c8r_tuning autotune(Accumulator* const* events, std::size_t n, int repetitions, double& best_ms) {
     static constexpr uint64_t kTeams[] = {256, 384, 512, 640};
     static constexpr uint64_t kChunks[] = {0, 32768, 131072, 524288};
+    static constexpr uint64_t kWindows[] = {2048, 1024, 512};
     c8r_tuning best{};
     best_ms = -1.;
     cudaEvent_t a = nullptr, b = nullptr;
     check(cudaEventCreate(&a), "event");
     check(cudaEventCreate(&b), "event");
+    auto trial = [&](c8r_tuning const& t) {
+      for (std::size_t i = 0; i < n; ++i) events[i]->set_tuning(t);
+      project(events, n, C8R_BATCH_KEEP_STAGED);  // warm
+      check(cudaEventRecord(a, stream_), "event");
+      for (int r = 0; r < repetitions; ++r) project(events, n, C8R_BATCH_KEEP_STAGED);
+      check(cudaEventRecord(b, stream_), "event");
+      check(cudaEventSynchronize(b), "event");
+      float ms = 0.f;
+      check(cudaEventElapsedTime(&ms, a, b), "event time");
+      double const per = ms / repetitions;
+      if (best_ms < 0. || per < best_ms) {
+        best_ms = per;
+        best = t;
+      }
+    };
     for (uint64_t team : kTeams) {
       for (uint64_t chunk : kChunks) {
         c8r_tuning t{};
         t.team_size = team;
         t.track_tile_size = chunk;
-        for (std::size_t i = 0; i < n; ++i) events[i]->set_tuning(t);
-        project(events, n, C8R_BATCH_KEEP_STAGED);  // warm
-        check(cudaEventRecord(a, stream_), "event");
-        for (int r = 0; r < repetitions; ++r) project(events, n, C8R_BATCH_KEEP_STAGED);
-        check(cudaEventRecord(b, stream_), "event");
-        check(cudaEventSynchronize(b), "event");
-        float ms = 0.f;
-        check(cudaEventElapsedTime(&ms, a, b), "event time");
-        double const per = ms / repetitions;
-        if (best_ms < 0. || per < best_ms) {
-          best_ms = per;
-          best = t;
-        }
+        trial(t);
       }
+    }
+    std::size_t longest = 0;
+    for (std::size_t i = 0; i < n; ++i) longest = std::max(longest, events[i]->largest_bins());
+    c8r_tuning const pair = best;
+    for (uint64_t window : kWindows) {
+      if (window >= longest) continue;
+      c8r_tuning t = pair;
+      t.observer_tile_size = window;
+      trial(t);
     }
     cudaEventDestroy(a);
     cudaEventDestroy(b);

@@ -322,12 +322,32 @@ int c8r_batch_create(void* stream, c8r_batch** batch);
 void c8r_batch_destroy(c8r_batch* batch);
 const char* c8r_batch_last_error(const c8r_batch* batch);
 int c8r_batch_project(c8r_batch* batch, c8r_accumulator* const* events, size_t count, int flags);
-/* Sweeps team size {256,384,512,640} x tracks per item {auto,32768,131072,524288}
- * on the staged events (repetitions timed runs each), applies the fastest to
- * every event, zeroes the traces the sweep wrote and returns it. */
+/* Sweeps the windowed kernel's tile space on the staged events (repetitions
+ * timed runs each): team size (track segments per stage) {256,384,512,640} x
+ * tracks per item {auto,32768,131072,524288} with the whole trace as bin
+ * window, then bin windows {2048,1024,512} shorter than the longest trace at
+ * the best pair (one antenna per CTA).  Applies the fastest to every event,
+ * zeroes the traces the sweep wrote and returns it (observer_tile_size 0:
+ * the whole trace). */
 int c8r_batch_autotune(c8r_batch* batch, c8r_accumulator* const* events, size_t count,
                        int repetitions, c8r_tuning* best, double* best_ms);
 int c8r_batch_graph_captures(const c8r_batch* batch, unsigned long long* captures);
+
+/* ---- Tuning cache -----------------------------------------------------------
+ * In the manner of the reference's c8-kokkos-tuning-v1 cache
+ * (corsika/kokkos/runtime/TuningCache.hpp:16-47): the autotuner's choice
+ * persisted as key=value lines ("c8radio-b200-tuning-v1"), keyed by the
+ * current device (name, compute capability, multiprocessors), driver and
+ * runtime versions, this library's version and a caller-chosen one-line
+ * workload label.  load sets *matched = 1 and *tuning (team_size,
+ * track_tile_size, observer_tile_size) only when the file exists and every
+ * key field equals the current one; a missing or non-matching file gives
+ * *matched = 0 (C8R_RUNTIME_ERROR when require_match), a malformed one
+ * C8R_RUNTIME_ERROR.  store writes a temporary file and renames it. */
+int c8r_tuning_cache_load(const char* path, const char* workload, int require_match, c8r_tuning* tuning,
+                          int* matched);
+int c8r_tuning_cache_store(const char* path, const char* workload, const c8r_tuning* tuning);
+const char* c8r_tuning_cache_last_error(void);
 
 /* ---- Producer-side input: track steps as columns ----------------------------
  * No counterpart in the reference, which reads the 752-byte records

@@ -125,3 +125,20 @@ def test_fixed_snapshot_merge_is_checked_before_writing(pkg):
         pkg.merge_fixed(destination, np.array([0, 0, 0, -(2 ** 62) - 1], np.int64))
     pkg.merge_fixed(destination, np.array([2, 1, 5, -(2 ** 62)], np.int64))
     assert destination.tolist() == [3, 2 ** 62 + 1, 0, -(2 ** 63)]
+
+
+def test_tuning_cache_files_without_a_gpu(pkg, tmp_path):
+    """The tuning cache (c8r_tuning_cache_load, in the manner of
+    TuningCache.cpp:101-129): a missing file is no match, an error only when a
+    match is required; a malformed file is an error either way.  Both are
+    decided before the device is queried."""
+    assert pkg.tuning_cache_load(tmp_path / "absent", "workload") is None
+    with pytest.raises(pkg.RadioError, match="no radio tuning cache"):
+        pkg.tuning_cache_load(tmp_path / "absent", "workload", require=True)
+    for name, text in (("no_equals", "format=c8radio-b200-tuning-v1\nbad line\n"),
+                       ("duplicate", "format=c8radio-b200-tuning-v1\nformat=x\n"),
+                       ("empty_key", "=value\n")):
+        path = tmp_path / name
+        path.write_text(text)
+        with pytest.raises(pkg.RadioError, match="tuning-cache"):
+            pkg.tuning_cache_load(path, "workload")

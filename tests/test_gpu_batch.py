@@ -81,6 +81,9 @@ def test_autotune_then_batch_is_exact(pkg, oracle, showers, torch_cuda):
     batch = pkg.RadioBatch(stream=stream.cuda_stream)
     best, ms = batch.autotune(accs, repetitions=1)
     assert best.team_size in (256, 384, 512, 640) and ms > 0
+    # bin windows shorter than the 1024-bin traces are part of the sweep; a
+    # chosen 512-bin window sends bins past it to checked global atomics
+    assert best.observer_tile_size in (0, 512)
     batch.project(accs)
     for (wl, records), acc in zip(events, accs):
         coreas, zhs, _ = acc.download_fixed()
@@ -99,3 +102,25 @@ def test_staged_tracks_project_at_download(pkg, oracle, showers, torch_cuda):
     want = oracle.restatement().project(showers.make_config(wl), records, threads=8)
     assert np.array_equal(coreas, want[0]) and np.array_equal(zhs, want[1])
     acc.close()
+
+
+def test_tuning_cache_round_trip(pkg, tmp_path, torch_cuda):
+    """A stored tuning loads back for the same device, build and workload
+    label, and only for them (TuningCache.cpp:65-82: every key field must
+    match)."""
+    path = tmp_path / "radio.tuning"
+    assert pkg.tuning_cache_load(path, "batched 64 events") is None
+    chosen = pkg.TuningParameters(team_size=512, track_tile_size=131072, observer_tile_size=1024)
+    pkg.tuning_cache_store(path, "batched 64 events", chosen)
+    text = path.read_text()
+    assert text.startswith("format=c8radio-b200-tuning-v1\n") and "device_name=" in text
+    got = pkg.tuning_cache_load(path, "batched 64 events", require=True)
+    assert (got.team_size, got.track_tile_size, got.observer_tile_size) == (512, 131072, 1024)
+    assert pkg.tuning_cache_load(path, "another workload") is None
+    with pytest.raises(pkg.RadioError, match="does not match"):
+        pkg.tuning_cache_load(path, "another workload", require=True)
+    path.write_text(text.replace("multiprocessors=", "multiprocessors=1"))
+    assert pkg.tuning_cache_load(path, "batched 64 events") is None
+    path.write_text(text.replace("team_size=512", "team_size=5x"))
+    with pytest.raises(pkg.RadioError, match="not a count"):
+        pkg.tuning_cache_load(path, "batched 64 events")
