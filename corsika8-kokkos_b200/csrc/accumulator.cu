@@ -681,7 +681,7 @@ class Accumulator {
     if (!enabled() || count == 0 || count <= capacity_) return;
     if (capacity_ > std::numeric_limits<std::size_t>::max() / 2)
       throw std::length_error("radio track capacity overflow");
-    std::size_t const grown = capacity_ == 0 ? count : std::max(count, 2 * capacity_);
+    std::size_t const grown = track_capacity(capacity_ == 0 ? count : std::max(count, 2 * capacity_));
     std::size_t const old_bytes = tracks_.bytes();
     std::size_t const new_bytes = checked_mul(checked_mul(grown, kTrackDoubles), sizeof(double));
     retained = current - old_bytes + new_bytes;
@@ -858,11 +858,12 @@ class Accumulator {
     if (capacity_ >= count) return;
     if (capacity_ > std::numeric_limits<std::size_t>::max() / 2)
       throw std::length_error("radio track capacity overflow");
-    std::size_t const grown = capacity_ == 0 ? count : std::max(count, 2 * capacity_);
+    // whole tiles of the workspace layout (track_capacity)
+    std::size_t const grown = track_capacity(capacity_ == 0 ? count : std::max(count, 2 * capacity_));
     DeviceBuffer<double> fresh;
     fresh.allocate(checked_mul(grown, kTrackDoubles));
-    if (staged_ != 0)  // keep the tracks staged so far
-      check(cudaMemcpyAsync(fresh.ptr, tracks_.ptr, staged_ * kTrackDoubles * sizeof(double),
+    if (staged_ != 0)  // keep the tiles staged so far (capacity_ is whole tiles)
+      check(cudaMemcpyAsync(fresh.ptr, tracks_.ptr, track_capacity(staged_) * kTrackDoubles * sizeof(double),
                             cudaMemcpyDeviceToDevice, stream_),
             "staged track copy");
     // earlier projections may still read the old workspace
@@ -903,6 +904,7 @@ class Accumulator {
       std::size_t const target_chunks = std::max<std::size_t>(1, (16 * ctas + per_chunk - 1) / std::max<uint32_t>(per_chunk, 1));
       chunk = std::max<std::size_t>(8192, (count + target_chunks - 1) / target_chunks);
       chunk = std::max<std::size_t>(chunk, std::min<std::size_t>((count + 7) / 8, 262144));
+      chunk = track_capacity(chunk);  // items start on a track tile
     }
     chunk = std::min<std::size_t>(chunk, 0x7fffffffu);
     ev.chunk_size = static_cast<uint32_t>(chunk);

@@ -56,7 +56,9 @@ constexpr std::size_t kObserversOffset = kTableOffset + kMaxTableEntries * sizeo
 constexpr std::size_t kDeferredOffset = kObserversOffset + kMaxObservers * sizeof(ObserverCache);
 constexpr std::size_t kDeferredEntries = std::size_t(2) << 20;
 constexpr std::size_t kTracksOffset = kDeferredOffset + kDeferredEntries * sizeof(unsigned);
-constexpr std::size_t kTrackCapacity = (kScratchBytes - kTracksOffset) / kTrackBytes;
+// whole tiles of the track workspace layout (c8r::track_column)
+constexpr std::size_t kTrackCapacity =
+    (kScratchBytes - kTracksOffset) / kTrackBytes / c8r::kTrackTile * c8r::kTrackTile;
 static_assert(sizeof(DeviceCounters) <= kSlotOffset - kCountersOffset, "scratch layout");
 static_assert(kObserversOffset % 256 == 0 && kDeferredOffset % 256 == 0 && kTracksOffset % 256 == 0,
               "scratch alignment");

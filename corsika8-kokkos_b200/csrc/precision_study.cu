@@ -442,22 +442,21 @@ __device__ __forceinline__ unsigned long long lane_sum(unsigned long long v) {
 }
 
 __device__ __forceinline__ Track study_track(const double* base, uint64_t i) {
-  const double* r = base + i * kTrackDoubles;
   Track t;
-  t.sx = r[kSx];
-  t.sy = r[kSy];
-  t.sz = r[kSz];
-  t.ex = r[kEx];
-  t.ey = r[kEy];
-  t.ez = r[kEz];
-  t.ts = r[kTs];
-  t.te = r[kTe];
-  t.bx = r[kBx];
-  t.by = r[kBy];
-  t.bz = r[kBz];
-  t.length = r[kLen];
-  t.beta_module = r[kBmod];
-  t.constant = r[kConst];
+  t.sx = track_field(base, i, kSx);
+  t.sy = track_field(base, i, kSy);
+  t.sz = track_field(base, i, kSz);
+  t.ex = track_field(base, i, kEx);
+  t.ey = track_field(base, i, kEy);
+  t.ez = track_field(base, i, kEz);
+  t.ts = track_field(base, i, kTs);
+  t.te = track_field(base, i, kTe);
+  t.bx = track_field(base, i, kBx);
+  t.by = track_field(base, i, kBy);
+  t.bz = track_field(base, i, kBz);
+  t.length = track_field(base, i, kLen);
+  t.beta_module = track_field(base, i, kBmod);
+  t.constant = track_field(base, i, kConst);
   return t;
 }
 

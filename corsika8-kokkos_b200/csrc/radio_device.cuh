@@ -71,21 +71,51 @@ struct Track {
   double length, beta_module, constant;
 };
 
-// Track workspace: one 192-byte record of 24 doubles per track.  The first
+// Track workspace: a record of 24 doubles (192 bytes) per track.  The first
 // 16: start xyz, end xyz, t_start, t_end, beta xyz, length, |beta|, charge
 // constant, n_dst at the start point, one spare.  When every observer of the
 // event shares one destination row (SourceTerms below), the last 8 hold the
 // propagation terms of four source points, precomputed at ingest -- start,
 // end, the ZHS segment midpoint (start + (start + (end - start))) / 2 and the
-// CoREAS near-cone midpoint (start + end) / 2, each as (factor, n_src).  (One interleaved
-// record measured faster for the CoREAS kernel than a separate 128-byte
-// record of its fields: 61.7 against 64.3 ms on the 1e7 x 160 workload.)
+// CoREAS near-cone midpoint (start + end) / 2, each as (factor, n_src).
+// Records are stored in tiles (track_column below).
 enum TrackField : int {
   kSx = 0, kSy, kSz, kEx, kEy, kEz, kTs, kTe, kBx, kBy, kBz, kLen, kBmod, kConst, kNdstStart, kSpare,
   kFactorStart, kNsrcStart, kFactorEnd, kNsrcEnd, kFactorMidZhs, kNsrcMidZhs, kFactorMidCoreas,
   kNsrcMidCoreas, kTrackDoubles
 };
 static_assert(kTrackDoubles == 24, "192-byte track records");
+
+// The workspace holds tiles of kTrackTile consecutive tracks (6144 bytes): in
+// a tile, column k of the records (doubles 2k and 2k + 1, one 16-byte double2)
+// is contiguous over the tile's 32 tracks.  The 32 lanes of a warp that read
+// one column of 32 consecutive tracks then read 512 contiguous bytes (4 cache
+// lines) where interleaved 192-byte records put every lane on its own line;
+// the projection kernels' track loads were bound by the L1 data pipe's
+// wavefronts with interleaved records.  A workspace is a whole number of tiles
+// (track_capacity), so every column of a track below the capacity is inside it.
+constexpr unsigned kTrackTile = 32;
+constexpr unsigned kTrackColumns = kTrackDoubles / 2;
+
+// Index (in double2 units) of column k of track i.
+__host__ __device__ __forceinline__ uint64_t track_column(uint64_t i, unsigned k) {
+  return (i / kTrackTile) * (kTrackTile * kTrackColumns) + k * kTrackTile + (i % kTrackTile);
+}
+// Column 0 of track i; column k is at [k * kTrackTile].
+__host__ __device__ __forceinline__ double2 const* track_ref(double const* base, uint64_t i) {
+  return reinterpret_cast<double2 const*>(base) + track_column(i, 0);
+}
+__host__ __device__ __forceinline__ double2* track_ref(double* base, uint64_t i) {
+  return reinterpret_cast<double2*>(base) + track_column(i, 0);
+}
+// Field f of track i.
+__host__ __device__ __forceinline__ double track_field(double const* base, uint64_t i, int f) {
+  return base[2 * track_column(i, static_cast<unsigned>(f) / 2) + (f & 1)];
+}
+// Tracks a workspace for n tracks holds: n rounded up to whole tiles.
+__host__ __device__ constexpr uint64_t track_capacity(uint64_t n) {
+  return (n + kTrackTile - 1) / kTrackTile * kTrackTile;
+}
 
 struct Path {
   double time, n_src, n_dst, dist, kx, ky, kz;

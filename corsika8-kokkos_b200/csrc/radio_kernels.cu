@@ -908,9 +908,10 @@ __device__ __forceinline__ bool zhs_common(Track const& t, Propagation const& p,
 __device__ __forceinline__ Track load_track(const double* __restrict__ base, uint64_t stride,
                                             uint64_t i) {
   (void)stride;
-  double2 const* r = reinterpret_cast<double2 const*>(base + i * kTrackDoubles);
-  double2 const a = __ldg(r + 0), b = __ldg(r + 1), c = __ldg(r + 2), d = __ldg(r + 3);
-  double2 const e = __ldg(r + 4), f = __ldg(r + 5), g = __ldg(r + 6);
+  double2 const* r = track_ref(base, i);
+  constexpr unsigned T = kTrackTile;
+  double2 const a = __ldg(r + 0 * T), b = __ldg(r + 1 * T), c = __ldg(r + 2 * T), d = __ldg(r + 3 * T);
+  double2 const e = __ldg(r + 4 * T), f = __ldg(r + 5 * T), g = __ldg(r + 6 * T);
   Track t;
   t.sx = a.x;
   t.sy = a.y;
@@ -929,7 +930,8 @@ __device__ __forceinline__ Track load_track(const double* __restrict__ base, uin
   return t;
 }
 
-// A track staged in shared memory (plain loads: __ldg reads the global space only).
+// A track staged in shared memory as one interleaved 192-byte record (plain
+// loads: __ldg reads the global space only).
 __device__ __forceinline__ Track load_staged_track(double const* base, unsigned i) {
   double2 const* r = reinterpret_cast<double2 const*>(base + i * kTrackDoubles);
   double2 const a = r[0], b = r[1], c = r[2], d = r[3], e = r[4], f = r[5], g = r[6];
@@ -1067,14 +1069,15 @@ __global__ void __launch_bounds__(256) ingest_kernel(
   base = __shfl_sync(0xffffffffu, base, 0);
   if (valid) {
     uint64_t const j = base + __popc(ballot & ((1u << lane) - 1u));
-    double2* r = reinterpret_cast<double2*>(tracks + j * kTrackDoubles);
-    r[0] = make_double2(t.sx, t.sy);
-    r[1] = make_double2(t.sz, t.ex);
-    r[2] = make_double2(t.ey, t.ez);
-    r[3] = make_double2(t.ts, t.te);
-    r[4] = make_double2(t.bx, t.by);
-    r[5] = make_double2(t.bz, t.length);
-    r[6] = make_double2(t.beta_module, t.constant);
+    double2* r = track_ref(tracks, j);
+    constexpr unsigned T = kTrackTile;
+    r[0 * T] = make_double2(t.sx, t.sy);
+    r[1 * T] = make_double2(t.sz, t.ex);
+    r[2 * T] = make_double2(t.ey, t.ez);
+    r[3 * T] = make_double2(t.ts, t.te);
+    r[4 * T] = make_double2(t.bx, t.by);
+    r[5 * T] = make_double2(t.bz, t.length);
+    r[6 * T] = make_double2(t.beta_module, t.constant);
     if (terms.enabled) {
       // the source points of the windowed kernels, with the reference's own
       // arithmetic: the ZHS segment of an undivided track ends at
@@ -1086,13 +1089,13 @@ __global__ void __launch_bounds__(256) ingest_kernel(
       SourceTerms const e = source_terms(p, d, t.ez);
       SourceTerms const mz = source_terms(p, d, (t.sz + (t.sz + (t.ez - t.sz))) * 0.5);
       SourceTerms const mc = source_terms(p, d, (t.sz + t.ez) * 0.5);
-      r[7] = make_double2(s.n_dst, 0.);
-      r[8] = make_double2(s.factor, s.n_src);
-      r[9] = make_double2(e.factor, e.n_src);
-      r[10] = make_double2(mz.factor, mz.n_src);
-      r[11] = make_double2(mc.factor, mc.n_src);
+      r[7 * T] = make_double2(s.n_dst, 0.);
+      r[8 * T] = make_double2(s.factor, s.n_src);
+      r[9 * T] = make_double2(e.factor, e.n_src);
+      r[10 * T] = make_double2(mz.factor, mz.n_src);
+      r[11 * T] = make_double2(mc.factor, mc.n_src);
     } else {
-      r[7] = make_double2(0., 0.);
+      r[7 * T] = make_double2(0., 0.);
     }
   }
   if (lane == 0 && ballot) atomicAdd(&counters->valid_tracks, static_cast<unsigned long long>(__popc(ballot)));
@@ -1249,11 +1252,13 @@ __global__ void __launch_bounds__(kTileThreads) tiled_kernel(const __grid_consta
     uint64_t const track_base = (tile / observer_tiles) * kTileTracks;
     uint64_t const observer_base = (tile % observer_tiles) * kTileObservers;
     __syncthreads();  // the previous tile's reads are done
-    for (unsigned i = threadIdx.x; i < kTileTracks * kTrackDoubles / 2; i += blockDim.x) {
-      uint64_t const row = track_base + i / (kTrackDoubles / 2);
-      reinterpret_cast<double2*>(tracks)[i] =
-          row < valid ? __ldg(reinterpret_cast<double2 const*>(ev.tracks) + track_base * (kTrackDoubles / 2) + i)
-                      : make_double2(0., 0.);
+    // column-major over the tile's tracks: consecutive threads read
+    // consecutive tracks of one column (kTileTracks divides kTrackTile)
+    for (unsigned i = threadIdx.x; i < kTileTracks * kTrackColumns; i += blockDim.x) {
+      unsigned const k = i / kTileTracks, lane = i % kTileTracks;
+      uint64_t const row = track_base + lane;
+      reinterpret_cast<double2*>(tracks)[lane * kTrackColumns + k] =
+          row < valid ? __ldg(track_ref(ev.tracks, row) + k * kTrackTile) : make_double2(0., 0.);
     }
     constexpr unsigned kWords = sizeof(ObserverCache) / sizeof(double2);
     for (int a = 0; a < 2; ++a) {
@@ -1383,9 +1388,9 @@ __device__ __noinline__ Counts zhs_drain(const double* __restrict__ tracks, uint
     if (s < segments) {
       // velocity and charge constant read again each step (L1): fewer
       // registers held across the warp's steps
-      double2 const* r = reinterpret_cast<double2 const*>(tracks + row * kTrackDoubles);
+      double2 const* r = track_ref(tracks, row);
       asm volatile("" : "+l"(r));
-      double2 const e = __ldg(r + 4), f = __ldg(r + 5), g = __ldg(r + 6);
+      double2 const e = __ldg(r + 4 * kTrackTile), f = __ldg(r + 5 * kTrackTile), g = __ldg(r + 6 * kTrackTile);
       Track t;
       t.bx = e.x;
       t.by = e.y;
@@ -1423,9 +1428,10 @@ __device__ __noinline__ Counts coreas_drain_pair(const double* __restrict__ trac
                                                  Sink sink) {
   Counts c;
   if (kPre) {
-    double2 const* r = reinterpret_cast<double2 const*>(tracks + row * kTrackDoubles);
-    double2 const n = __ldg(r + kNdstStart / 2), s = __ldg(r + kFactorStart / 2), e = __ldg(r + kFactorEnd / 2),
-                  m = __ldg(r + kFactorMidCoreas / 2);
+    double2 const* r = track_ref(tracks, row);
+    constexpr unsigned T = kTrackTile;
+    double2 const n = __ldg(r + kNdstStart / 2 * T), s = __ldg(r + kFactorStart / 2 * T),
+                  e = __ldg(r + kFactorEnd / 2 * T), m = __ldg(r + kFactorMidCoreas / 2 * T);
     SourceTerms const pre[3] = {{s.x, s.y, n.x}, {e.x, e.y, 0.}, {m.x, m.y, 0.}};
     coreas_pair<kFixed, Amp, Sink, true>(load_track(tracks, 0, row), p, o, sink, c, pre);
   } else {
@@ -1439,13 +1445,15 @@ __device__ __noinline__ Counts coreas_drain_pair(const double* __restrict__ trac
 template <int kAlgorithm>
 __device__ __forceinline__ void load_source_terms(const double* __restrict__ base, uint64_t i,
                                                   SourceTerms& a, SourceTerms& b) {
-  double2 const* r = reinterpret_cast<double2 const*>(base + i * kTrackDoubles);
+  double2 const* r = track_ref(base, i);
+  constexpr unsigned T = kTrackTile;
   if (kAlgorithm == 0) {
-    double2 const n = __ldg(r + kNdstStart / 2), s = __ldg(r + kFactorStart / 2), e = __ldg(r + kFactorEnd / 2);
+    double2 const n = __ldg(r + kNdstStart / 2 * T), s = __ldg(r + kFactorStart / 2 * T),
+                  e = __ldg(r + kFactorEnd / 2 * T);
     a = SourceTerms{s.x, s.y, n.x};
     b = SourceTerms{e.x, e.y, 0.};
   } else {
-    double2 const m = __ldg(r + kFactorMidZhs / 2);
+    double2 const m = __ldg(r + kFactorMidZhs / 2 * T);
     a = SourceTerms{m.x, m.y, 0.};
   }
 }

@@ -119,8 +119,9 @@ inline uint64_t append_work(WorkPlan& plan, EventPlan ev, uint64_t ctas, bool fi
   uint64_t const per = ev.observer_count[plan.algorithm];
   if (per == 0 || ev.chunks == 0 || plan.event_count >= kPlanEntries) return 0;
   uint64_t const big = ev.chunk_size;
-  uint64_t const small = (big + kSplit - 1) / kSplit > kMinTailChunk ? (big + kSplit - 1) / kSplit
-                                                                     : kMinTailChunk;
+  // whole track tiles, so that short items start on a tile as long ones do
+  uint64_t const small = track_capacity((big + kSplit - 1) / kSplit > kMinTailChunk ? (big + kSplit - 1) / kSplit
+                                                                                    : kMinTailChunk);
   uint64_t head = ev.chunks;
   if (fine_tail && plan.event_count + 2 <= kPlanEntries && small < big) {
     uint64_t const short_items = (2 * ctas + per - 1) / per;

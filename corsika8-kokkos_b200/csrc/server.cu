@@ -201,7 +201,7 @@ class Server {
     check(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, device_), "SM count");
     max_window_ = windowed_max_bins(device_);
     if (max_window_ <= 0) throw server_cuda_error("windowed radio kernel does not fit on this device");
-    block_bytes_ = kGranule + block_tracks_ * kTrackDoubles * sizeof(double);
+    block_bytes_ = kGranule + track_capacity(block_tracks_) * kTrackDoubles * sizeof(double);
     if (options.budget_bytes < block_bytes_)
       throw std::invalid_argument("server budget is smaller than one kinematics block");
     arena_.reserve(options.budget_bytes);

@@ -82,7 +82,7 @@ _cache: dict = {}
 def restatement() -> _Backend:
     if "o" not in _cache:
         if not RESTATEMENT.exists():
-            build(reference=False)
+            build()
         _cache["o"] = _Backend(RESTATEMENT, "c8o")
         lib = _cache["o"].lib
         lib.c8o_nearest_bin.restype = C.c_double
