@@ -906,7 +906,7 @@ class Accumulator {
       chunk = std::max<std::size_t>(chunk, std::min<std::size_t>((count + 7) / 8, 262144));
       chunk = track_capacity(chunk);  // items start on a track tile
     }
-    chunk = std::min<std::size_t>(chunk, 0x7fffffffu);
+    chunk = std::min<std::size_t>(chunk, kMaxChunkTracks);
     ev.chunk_size = static_cast<uint32_t>(chunk);
     ev.chunks = static_cast<uint32_t>((count + chunk - 1) / chunk);
     ev.first_track = 0;

@@ -376,9 +376,13 @@ __device__ __forceinline__ FastPath filtered_path(Propagation const& p, Observer
 // margin).  The branches (near-Cherenkov |doppler| < 1e-3, the sign test
 // doppler < 1e-9) are taken here only when that bound cannot move them, and
 // pairs with |doppler| < 1e-6 are left to the exact evaluation.  Sample times
-// are exact, so bins are the reference's.
+// are exact, so bins are the reference's.  Returns kCoreasDeposited, or the
+// deferral: kCoreasExact, or kCoreasNearCone with bit 0 the branch's
+// start-before-end order (sr < er, exact times), both decided exactly, so the
+// drain evaluates only the near-Cherenkov branch itself.
+constexpr int kCoreasDeposited = 0, kCoreasExact = 1, kCoreasNearCone = 2;
 template <bool kFixed, bool kFilter, bool kPre, class Amp, class Sink>
-__device__ __forceinline__ bool coreas_common(Track const& t, Propagation const& p,
+__device__ __forceinline__ int coreas_common(Track const& t, Propagation const& p,
                                               ObserverCache const& o, Sink& sink, Counts& c,
                                               SourceTerms const& pre_start, SourceTerms const& pre_end) {
   Path const ps = kPre ? propagate_with<true, kFilter>(pre_start, o, t.sx, t.sy, t.sz)
@@ -396,15 +400,15 @@ __device__ __forceinline__ bool coreas_common(Track const& t, Propagation const&
         fabs(pre) < 1.e-6 || fabs(post) < 1.e-6 ||
         (ps.n_dst > 1. && (fabs(fabs(pre) - kCoreasThreshold) <= err_pre ||
                            fabs(fabs(post) - kCoreasThreshold) <= err_post));
-    if (ambiguous) return false;
+    if (ambiguous) return kCoreasExact;
   } else {
     pre = doppler(ps.n_src, t.bx, t.by, t.bz, ps.kx, ps.ky, ps.kz);
     post = doppler(pe.n_src, t.bx, t.by, t.bz, pe.kx, pe.ky, pe.kz);
   }
-  if (ps.n_dst > 1. && (fabs(pre) < kCoreasThreshold || fabs(post) < kCoreasThreshold))
-    return false;
   double sr = t.ts + ps.time;
   double er = t.te + pe.time;
+  if (ps.n_dst > 1. && (fabs(pre) < kCoreasThreshold || fabs(post) < kCoreasThreshold))
+    return kCoreasNearCone | (sr < er ? 1 : 0);
   Vec3<Amp> const beta{static_cast<Amp>(t.bx), static_cast<Amp>(t.by), static_cast<Amp>(t.bz)};
   Vec3<Amp> const ks{static_cast<Amp>(ps.kx), static_cast<Amp>(ps.ky), static_cast<Amp>(ps.kz)};
   Vec3<Amp> const ke{static_cast<Amp>(pe.kx), static_cast<Amp>(pe.ky), static_cast<Amp>(pe.kz)};
@@ -426,7 +430,7 @@ __device__ __forceinline__ bool coreas_common(Track const& t, Propagation const&
   }
   add_sample<false, kFixed>(o, sink, sr, fstart, c.coreas, c.overflows, c.mag);
   add_sample<false, kFixed>(o, sink, er, fend, c.coreas, c.overflows, c.mag);
-  return true;
+  return kCoreasDeposited;
 }
 
 // Intermediate ZHS bins binned index by index with the reference's own
@@ -789,6 +793,110 @@ __device__ __forceinline__ void deposit_staged(StagedSegment<Amp>* staging,
         }
         deposit_bin<kFixed>(sink, bin, make_deposit<kFixed>(grid, scaled(g.perp, scale)), c.zhs,
                             c.overflows, c.mag);
+      }
+    }
+  }
+  __syncwarp();
+}
+
+// The fixed-point value of one component, as to_fixed computes it.
+__device__ __forceinline__ long long fixed_value(float v, ObserverCache const& grid) {
+  return __float2ll_rn(v * grid.fixed_scale_f);
+}
+__device__ __forceinline__ long long fixed_value(double v, ObserverCache const& grid) {
+  return __double2ll_rn(v * grid.fixed_scale);
+}
+
+// The owner's half of the unchecked deposit of its staged segment (fixed
+// point, the whole trace in the window, whose adds are not checked): shows
+// once for the segment that every sample converts -- each component's
+// |(p_c scale) fixed_scale| is at most max|p_c| max|scale| fixed_scale (1 +
+// 2^-22), kept below 2^62 -- counts the samples as contributions and adds
+// an upper bound of their |components| to the window bound (each factor's
+// roundings, at most nine of 2^-24, inside the 2^-20 margin).  The deposit
+// then converts and adds each sample with no check.  Returns false when a
+// sample might not convert (huge or non-finite values) or in the diagnostic
+// count-samples mode: the pair then goes to the checked drain.
+template <class Amp>
+__device__ __forceinline__ bool account_staged(StagedSegment<Amp> const& seg, ObserverCache const& o,
+                                               Counts& c) {
+  uint32_t const samples = seg.count + ((seg.flags >> 1) & 1u);
+  if (samples == 0u) return true;
+  if (o.count_samples) return false;
+  bool const has_first = (seg.flags & 1u) != 0u;
+  uint32_t const mids = seg.count - (has_first ? 1u : 0u);
+  Amp const zero = static_cast<Amp>(0);
+  Amp const af = has_first ? fabs(seg.first) : zero;
+  Amp const am = mids ? fabs(seg.mid) : zero;
+  Amp const al = (seg.flags & 2u) ? fabs(seg.last) : zero;
+  Amp const px = fabs(seg.perp.x), py = fabs(seg.perp.y), pz = fabs(seg.perp.z);
+  Amp const fs = sizeof(Amp) == sizeof(float) ? static_cast<Amp>(o.fixed_scale_f) : static_cast<Amp>(o.fixed_scale);
+  Amp const largest = fmax(fmax(px, py), pz) * fmax(fmax(af, am), al) * fs;
+  if (!(largest < static_cast<Amp>(0x1p62))) return false;  // also NaN and infinities
+  Amp const sum = (af + am * static_cast<Amp>(mids) + al) * (px + py + pz) * fs *
+                  static_cast<Amp>(1. + 0x1p-20);
+  c.zhs += samples;
+  c.mag += sizeof(Amp) == sizeof(float) ? static_cast<float>(sum)
+                                        : __double2float_ru(static_cast<double>(sum));
+  return true;
+}
+
+// The unchecked deposit of a warp's staged segments: deposit_staged's
+// redistribution (every lane takes two bins of the flattened list per step),
+// each sample converted and added to the window with no check, its counts
+// and bound already taken by account_staged.  Every bin is below the trace's
+// bins, which the window holds whole.
+template <class Amp>
+__device__ __forceinline__ void deposit_unchecked(StagedSegment<Amp>* staging, StagedSegment<Amp> const& seg,
+                                                  ObserverCache const& o, WindowSink const& sink) {
+  unsigned const lane = threadIdx.x & 31u;
+  uint32_t const cnt = seg.count + ((seg.flags >> 1) & 1u);
+  uint32_t incl = cnt;
+#pragma unroll
+  for (unsigned d = 1; d < 32u; d <<= 1) {
+    uint32_t const v = __shfl_up_sync(0xffffffffu, incl, d);
+    if (lane >= d) incl += v;
+  }
+  uint32_t const total = __shfl_sync(0xffffffffu, incl, 31);
+  if (total == 0u) return;
+  staging[lane] = seg;
+  __syncwarp();
+  uint32_t const before_mine = incl - cnt;
+  ObserverCache grid;  // the converting fields in registers
+  grid.fixed_scale = o.fixed_scale;
+  grid.fixed_scale_f = o.fixed_scale_f;
+  unsigned long long* const win = sink.win;
+  uint32_t const width = sink.width;
+  // kPer bins per lane per step, their owner searches interleaved
+  constexpr int kPer = sizeof(Amp) == sizeof(float) ? 2 : 4;  // measured best of 2 and 4
+  for (uint32_t base = 0; base < total; base += 32u * kPer) {
+    uint32_t owner[kPer], before[kPer];
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) owner[u] = 0u;
+#pragma unroll
+    for (uint32_t step = 16; step >= 1u; step >>= 1) {
+#pragma unroll
+      for (int u = 0; u < kPer; ++u) {
+        uint32_t const v = __shfl_sync(0xffffffffu, incl, owner[u] + step - 1u);
+        if (v <= base + lane + 32u * u) owner[u] += step;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) before[u] = __shfl_sync(0xffffffffu, before_mine, owner[u] & 31u);
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) {
+      uint32_t const j = base + lane + 32u * u;
+      if (j < total) {
+        StagedSegment<Amp> const& g = staging[owner[u]];
+        uint32_t const k = j - before[u];
+        bool const last = k >= g.count;
+        uint32_t const bin = last ? g.last_bin : g.start + k;
+        Amp const scale = last ? g.last : ((k == 0u && (g.flags & 1u)) ? g.first : g.mid);
+        Vec3<Amp> const v = scaled(g.perp, scale);
+        unsigned long long* const w = win + bin;
+        atomicAdd(w, static_cast<unsigned long long>(fixed_value(v.x, grid)));
+        atomicAdd(w + width, static_cast<unsigned long long>(fixed_value(v.y, grid)));
+        atomicAdd(w + 2 * width, static_cast<unsigned long long>(fixed_value(v.z, grid)));
       }
     }
   }
@@ -1421,12 +1529,22 @@ __device__ __noinline__ Counts zhs_drain(const double* __restrict__ tracks, uint
 }
 
 // A deferred CoREAS pair of the windowed kernel, loaded and evaluated exactly
-// out of line (the caller passes the row, not the 112-byte track).
+// out of line (the caller passes the row, not the 112-byte track).  `hint`
+// (kCoreasNearCone, as the track loop decided it, else 0): the pair takes the
+// near-Cherenkov branch in the order of bit 0, evaluated here directly.
 template <bool kFixed, class Amp, bool kPre, class Sink>
 __device__ __noinline__ Counts coreas_drain_pair(const double* __restrict__ tracks, uint64_t row,
-                                                 Propagation const& p, ObserverCache const& o,
-                                                 Sink sink) {
+                                                 unsigned hint, Propagation const& p,
+                                                 ObserverCache const& o, Sink sink) {
   Counts c;
+  if (hint & static_cast<unsigned>(kCoreasNearCone)) {
+    SourceTerms mid{};
+    if (kPre) {
+      double2 const m = __ldg(track_ref(tracks, row) + kFactorMidCoreas / 2 * kTrackTile);
+      mid = SourceTerms{m.x, m.y, 0.};
+    }
+    return coreas_near_cone<kFixed, Amp, kPre>(load_track(tracks, 0, row), p, o, sink, (hint & 1u) != 0u, mid);
+  }
   if (kPre) {
     double2 const* r = track_ref(tracks, row);
     constexpr unsigned T = kTrackTile;
@@ -1541,6 +1659,7 @@ __global__ void __launch_bounds__(kAlgorithm == 1 ? kZhsThreadsMax : kWindowThre
       for (uint64_t base = begin; base < end; base += blockDim.x) {
         uint64_t const i = base + threadIdx.x;
         bool deferred = false;
+        unsigned hint = 0u;  // CoREAS: the near-Cherenkov decision, in the list entry's top bits
         StagedSegment<Amp> seg;
         seg.count = 0u;
         seg.flags = 0u;
@@ -1548,20 +1667,34 @@ __global__ void __launch_bounds__(kAlgorithm == 1 ? kZhsThreadsMax : kWindowThre
           Track const t = load_track(ev.tracks, ev.stride, i);
           SourceTerms pa{}, pb{};
           if (kPre) load_source_terms<kAlgorithm>(ev.tracks, i, pa, pb);
-          bool const done =
-              kAlgorithm == 0
-                  ? coreas_common<kFixed, kFilter, kPre, Amp>(t, ev.propagation, o, sink, c, pa, pb)
-                  : zhs_common<kFilter, kPre, Amp>(t, ev.propagation, o, c, seg, pa);
-          deferred = !done;
+          if constexpr (kAlgorithm == 0) {
+            int const code = coreas_common<kFixed, kFilter, kPre, Amp>(t, ev.propagation, o, sink, c, pa, pb);
+            deferred = code != kCoreasDeposited;
+            hint = code >= kCoreasNearCone ? static_cast<unsigned>(code) << kDeferredHintShift : 0u;
+          } else {
+            deferred = !zhs_common<kFilter, kPre, Amp>(t, ev.propagation, o, c, seg, pa);
+          }
         }
-        if (kAlgorithm == 1) deposit_staged<kFixed>(staging, seg, o, sink, c);
+        if (kAlgorithm == 1) {
+          if (kFixed && sink.unchecked) {
+            if (!deferred && !account_staged(seg, o, c)) {
+              seg.count = 0u;
+              seg.flags = 0u;
+              deferred = true;
+              c.subtracks -= 1ull;  // the drain counts the pair's subtracks
+            }
+            deposit_unchecked(staging, seg, o, sink);
+          } else {
+            deposit_staged<kFixed>(staging, seg, o, sink, c);
+          }
+        }
         unsigned const ballot = __ballot_sync(0xffffffffu, deferred);
         unsigned const rank = __popc(ballot & ((1u << lane) - 1u));
         if (ballot) {
           unsigned slot = 0;
           if (lane == 0) slot = atomicAdd(&deferred_total, static_cast<unsigned>(__popc(ballot)));
           slot = __shfl_sync(0xffffffffu, slot, 0);
-          if (deferred) deferred_list[slot + rank] = static_cast<unsigned>(i - begin);
+          if (deferred) deferred_list[slot + rank] = static_cast<unsigned>(i - begin) | hint;
         }
       }
       __syncthreads();
@@ -1573,8 +1706,9 @@ __global__ void __launch_bounds__(kAlgorithm == 1 ? kZhsThreadsMax : kWindowThre
           d = zhs_drain<kFixed, kFilter, Amp>(ev.tracks, begin, deferred_list + from, count,
                                               ev.propagation, o, sink, staging);
         } else if (lane < count) {
-          d = coreas_drain_pair<kFixed, Amp, kPre>(ev.tracks, begin + deferred_list[from + lane],
-                                             ev.propagation, o, sink);
+          unsigned const entry = deferred_list[from + lane];
+          d = coreas_drain_pair<kFixed, Amp, kPre>(ev.tracks, begin + (entry & kDeferredOffsetMask),
+                                                   entry >> kDeferredHintShift, ev.propagation, o, sink);
         }
         c.coreas += d.coreas;
         c.zhs += d.zhs;

@@ -99,6 +99,13 @@ struct WorkPlan {
   unsigned long long* reruns;
 };
 
+// A work item spans at most kMaxChunkTracks tracks: a deferred-list entry is
+// the pair's track offset in the item (its low 30 bits) and two bits of the
+// track loop's decision (CoREAS: the near-Cherenkov branch and its order).
+constexpr uint32_t kMaxChunkTracks = 1u << 30;
+constexpr unsigned kDeferredHintShift = 30;
+constexpr unsigned kDeferredOffsetMask = (1u << kDeferredHintShift) - 1u;
+
 // Entries per CTA of a launch's deferred lists: the plan's longest chunk.
 inline uint32_t deferred_list_stride(WorkPlan const& plan) {
   uint32_t stride = 0;

@@ -192,7 +192,7 @@ class Server {
     chunk_tracks_ = options.chunk_tracks ? options.chunk_tracks : 131072;
     round_pairs_ = options.round_pairs ? options.round_pairs : 1000000000ull;
     threads_ = options.team_size ? static_cast<int>(options.team_size) : kWindowThreads;
-    if (chunk_tracks_ == 0 || chunk_tracks_ > 0x7fffffffu || block_tracks_ % chunk_tracks_ != 0 ||
+    if (chunk_tracks_ == 0 || chunk_tracks_ > kMaxChunkTracks || block_tracks_ % chunk_tracks_ != 0 ||
         block_tracks_ / chunk_tracks_ > 0xffffffffu)
       throw std::invalid_argument("server block_tracks must be a multiple of chunk_tracks");
     if (threads_ > kWindowThreads || threads_ % 32 != 0 || threads_ < 32)

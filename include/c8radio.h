@@ -503,7 +503,7 @@ typedef struct c8r_server c8r_server;
 typedef struct c8r_server_options {
   uint64_t budget_bytes; /* HBM arena reserved at creation (events, blocks) */
   uint64_t block_tracks; /* tracks per kinematics block; 0 = 1048576 */
-  uint64_t chunk_tracks; /* tracks per work item; 0 = 131072 (divides block_tracks) */
+  uint64_t chunk_tracks; /* tracks per work item; 0 = 131072 (divides block_tracks, at most 2^30) */
   uint64_t round_pairs;  /* track-observer pairs per round; 0 = 1e9 */
   uint32_t team_size;    /* threads per windowed CTA; 0 = 640 (ZHS launches at most 384) */
   uint32_t reserved_[7];
