@@ -303,14 +303,36 @@ class Accumulator {
     return attributes.type == cudaMemoryTypeHost;
   }
 
+  // The bytes of a record the ingest reads: start.pid through start.weight
+  // and end.position through end.time (with the diagnostics' energy and
+  // directions), one span of 208 of the record's 752 bytes.  Host records are
+  // uploaded as that span alone, a pitched copy to the same offsets of the
+  // device staging records (whose other bytes the ingest never reads).
+  static constexpr std::size_t kUsedBegin = offsetof(c8r_lepton_transport_record, start);
+  static constexpr std::size_t kUsedEnd =
+      offsetof(c8r_lepton_transport_record, end) + offsetof(c8r_particle_state, time_s) + sizeof(double);
+  static_assert(offsetof(c8r_particle_state, weight) + sizeof(double) <=
+                    offsetof(c8r_lepton_transport_record, end) - offsetof(c8r_lepton_transport_record, start),
+                "start fields inside the span");
+  static_assert(kUsedEnd - kUsedBegin == 208, "208-byte span of the 752-byte record");
+
+  cudaError_t upload_used(c8r_lepton_transport_record* dst, c8r_lepton_transport_record const* src,
+                          std::size_t n, cudaStream_t stream) {
+    constexpr std::size_t kPitch = sizeof(c8r_lepton_transport_record);
+    return cudaMemcpy2DAsync(reinterpret_cast<unsigned char*>(dst) + kUsedBegin, kPitch,
+                             reinterpret_cast<unsigned char const*>(src) + kUsedBegin, kPitch,
+                             kUsedEnd - kUsedBegin, n, cudaMemcpyHostToDevice, stream);
+  }
+
   // Batches of host_batch_ records (the last one partial) copied from pinned
   // caller memory into a pair of device staging buffers (the copy of batch
   // k+1 overlaps the projection of batch k on the copy stream; a buffer is
   // free again once its ingest has run); returns after the last copy
   // completed.  The first batch is an eighth of host_batch_ and each next one
-  // a quarter longer, up to host_batch_: a copy takes about 0.8 of the
-  // projection of as many records, so every copy but the first stays hidden
-  // behind the projection of the batch before it, and the first is short.
+  // a quarter longer, up to host_batch_: a copy of the records' used spans
+  // takes about a quarter of the projection of as many records, so every copy
+  // but the first stays hidden behind the projection of the batch before it,
+  // and the first is short.
   void enqueue_pinned(c8r_lepton_transport_record const* records, std::size_t count) {
     if (!copy_stream_) {
       check(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking), "copy stream");
@@ -329,16 +351,14 @@ class Accumulator {
       c8r_lepton_transport_record* dst = k ? staging2_.ptr : staging_.ptr;
       // the staging buffer is free once the ingest that read it has run
       check(cudaStreamWaitEvent(copy_stream_, consumed_[k], 0), "wait");
-      check(cudaMemcpyAsync(dst, records + offset, n * sizeof(c8r_lepton_transport_record),
-                            cudaMemcpyHostToDevice, copy_stream_),
-            "host track upload");
+      check(upload_used(dst, records + offset, n, copy_stream_), "host track upload");
       check(cudaEventRecord(copy_done_[k], copy_stream_), "event");
       check(cudaStreamWaitEvent(stream_, copy_done_[k], 0), "wait");
       stage_device(dst, n, host_batch_);
       check(cudaEventRecord(consumed_[k], stream_), "event");
       project_staged(true);
       offset += n;
-      stats_.host_to_device_bytes += n * sizeof(c8r_lepton_transport_record);
+      stats_.host_to_device_bytes += n * (kUsedEnd - kUsedBegin);
       ++stats_.host_track_batches;
       stats_.host_tracks_enqueued += n;
     }
@@ -351,14 +371,12 @@ class Accumulator {
   void flush() {
     if (host_count_ == 0) return;
     std::size_t const n = host_count_;
-    check(cudaMemcpyAsync(staging_.ptr, host_[host_index_].ptr, n * sizeof(c8r_lepton_transport_record),
-                          cudaMemcpyHostToDevice, stream_),
-          "host track upload");
+    check(upload_used(staging_.ptr, host_[host_index_].ptr, n, stream_), "host track upload");
     check(cudaEventRecord(host_ready_[host_index_], stream_), "event");
     host_index_ ^= 1;
     host_count_ = 0;
     accumulate_device(staging_.ptr, n, staging_.count);
-    stats_.host_to_device_bytes += n * sizeof(c8r_lepton_transport_record);
+    stats_.host_to_device_bytes += n * (kUsedEnd - kUsedBegin);
     ++stats_.host_track_batches;
   }
 
