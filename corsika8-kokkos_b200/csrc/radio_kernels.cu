@@ -1408,11 +1408,32 @@ __global__ void __launch_bounds__(kTileThreads) tiled_kernel(const __grid_consta
 
 // ---------------------------------------------------------------- windowed
 constexpr int kWindowThreadsMax = kWindowThreads;
-// The ZHS kernel's live state needs more than 128 registers a thread: it runs
-// 384-thread CTAs (up to 168 registers, no spills).
-constexpr int kZhsThreadsMax = 384;
-// staging slots of the ZHS kernel: 32 per warp, sized for the FP64 amplitudes
-constexpr size_t kStagingBytes = (kZhsThreadsMax / 32) * 32 * sizeof(StagedSegment<double>);
+// Threads of a ZHS CTA.  Its drain's live state needs more registers than its
+// track loop (168 against 112 in FP32, 135 in FP64), so a CTA sized for the
+// drain runs 12 warps an SM.  Measured on the 1e7 x 160 workload (ms per ZHS
+// launch), FP32: 384 threads 96.8, 512 100.9, 576 97.3, 640 88.3, 768 79.9,
+// 832 82.7, 864 80.6 -- the track loop gains more from the warps than the
+// drain loses to its spills; FP64: 384 117.0, 480 128.5.
+constexpr int kZhsThreadsFloat = 768;
+constexpr int kZhsThreadsDouble = 384;
+template <class Amp>
+constexpr int zhs_threads_max() {
+  return sizeof(Amp) == sizeof(float) ? kZhsThreadsFloat : kZhsThreadsDouble;
+}
+// The ZHS block for a team of `threads`: the team when it is smaller than the
+// default team, else the largest block of the amplitude type.
+template <class Amp>
+constexpr int zhs_block(int threads) {
+  return threads < kWindowThreads ? (threads < zhs_threads_max<Amp>() ? threads : zhs_threads_max<Amp>())
+                                  : zhs_threads_max<Amp>();
+}
+// staging slots of the ZHS kernel: 32 per warp
+template <class Amp>
+constexpr size_t staging_bytes() {
+  return static_cast<size_t>(zhs_threads_max<Amp>()) * sizeof(StagedSegment<Amp>);
+}
+constexpr size_t kStagingBytes =
+    staging_bytes<float>() > staging_bytes<double>() ? staging_bytes<float>() : staging_bytes<double>();
 
 __device__ __forceinline__ uint32_t find_event(EventPlan const* events, uint32_t n, uint64_t item) {
   uint32_t lo = 0, hi = n;  // last event with first_item <= item
@@ -1577,7 +1598,7 @@ __device__ __forceinline__ void load_source_terms(const double* __restrict__ bas
 }
 
 template <bool kFixed, class Amp, int kAlgorithm, bool kPre>
-__global__ void __launch_bounds__(kAlgorithm == 1 ? kZhsThreadsMax : kWindowThreadsMax, 1)
+__global__ void __launch_bounds__(kAlgorithm == 1 ? zhs_threads_max<Amp>() : kWindowThreadsMax, 1)
     windowed_kernel(const __grid_constant__ WorkPlan plan) {
   extern __shared__ __align__(16) unsigned long long window[];
   __shared__ unsigned long long item_shared;
@@ -1842,9 +1863,10 @@ cudaError_t tiled_dispatch(EventPlan const& ev, uint64_t bound, bool coreas, boo
 }
 
 // window rows | (ZHS) per-warp staging slots
+template <class Amp>
 size_t windowed_smem_bytes(uint32_t window, int algorithm) {
   return static_cast<size_t>(window) * 3 * sizeof(unsigned long long) +
-         (algorithm == 1 ? kStagingBytes : 0);
+         (algorithm == 1 ? staging_bytes<Amp>() : 0);
 }
 
 // Every event of the plan carries precomputed source terms.
@@ -1857,12 +1879,12 @@ bool plan_precomputed(WorkPlan const& plan) {
 
 template <bool kFixed, class Amp, int kAlgorithm, bool kPre>
 cudaError_t windowed_launch(WorkPlan const& plan, int ctas, int threads, cudaStream_t stream) {
-  size_t const bytes = windowed_smem_bytes(plan.window, kAlgorithm);
+  size_t const bytes = windowed_smem_bytes<Amp>(plan.window, kAlgorithm);
   cudaError_t err = cudaFuncSetAttribute(windowed_kernel<kFixed, Amp, kAlgorithm, kPre>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(bytes));
   if (err != cudaSuccess) return err;
-  int const block = kAlgorithm == 1 && threads > kZhsThreadsMax ? kZhsThreadsMax : threads;
+  int const block = kAlgorithm == 1 ? zhs_block<Amp>(threads) : threads;
   windowed_kernel<kFixed, Amp, kAlgorithm, kPre><<<ctas, block, bytes, stream>>>(plan);
   return cudaGetLastError();
 }
@@ -1887,7 +1909,7 @@ template <bool kFixed, class Amp>
 int ctas_per_sm(int window, int threads) {
   int worst = 1 << 30;
   auto probe = [&](auto kernel, int block, int algorithm) {
-    size_t const bytes = windowed_smem_bytes(static_cast<uint32_t>(window), algorithm);
+    size_t const bytes = windowed_smem_bytes<Amp>(static_cast<uint32_t>(window), algorithm);
     cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
     int blocks = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, block, bytes) != cudaSuccess)
@@ -1896,9 +1918,8 @@ int ctas_per_sm(int window, int threads) {
   };
   probe(windowed_kernel<kFixed, Amp, 0, false>, threads, 0);
   probe(windowed_kernel<kFixed, Amp, 0, true>, threads, 0);
-  int const zhs_block = threads > kZhsThreadsMax ? kZhsThreadsMax : threads;
-  probe(windowed_kernel<kFixed, Amp, 1, false>, zhs_block, 1);
-  probe(windowed_kernel<kFixed, Amp, 1, true>, zhs_block, 1);
+  probe(windowed_kernel<kFixed, Amp, 1, false>, zhs_block<Amp>(threads), 1);
+  probe(windowed_kernel<kFixed, Amp, 1, true>, zhs_block<Amp>(threads), 1);
   return worst;
 }
 
