@@ -1024,7 +1024,7 @@ class Accumulator {
       append_work(plan, ev, ctas, true);
       if (ctas > plan.total_items) ctas = plan.total_items;
       plan.deferred_stride = deferred_list_stride(plan);
-      plan.deferred = deferred_lists(algorithm, ctas * plan.deferred_stride);
+      attach_deferred(plan, deferred_lists(algorithm, deferred_words(plan, ctas, fixed_)), ctas, fixed_);
       check(cudaMemsetAsync(plan.next_item, 0, sizeof(unsigned), s), "memset");
       cudaEvent_t b = nullptr, e = nullptr;
       if (timing_) {
@@ -1312,11 +1312,18 @@ class Batch {
         uint64_t const items = l.plan.total_items;
         if (ctas > items) ctas = items;
         l.plan.deferred_stride = deferred_list_stride(l.plan);
-        l.plan.deferred = deferred_lists(ctas * l.plan.deferred_stride);
         l.ctas = static_cast<int>(ctas);
         out.launches.push_back(l);
       }
     }
+    // one list storage for every launch (they run one after the other), sized
+    // for the largest before any launch points into it: growing it between
+    // launches would leave the earlier ones on the freed storage
+    uint64_t words = 0;
+    for (auto const& l : out.launches)
+      words = std::max(words, deferred_words(l.plan, static_cast<uint64_t>(l.ctas), fixed));
+    unsigned* const storage = deferred_lists(words);
+    for (auto& l : out.launches) attach_deferred(l.plan, storage, static_cast<uint64_t>(l.ctas), fixed);
     return out;
   }
 

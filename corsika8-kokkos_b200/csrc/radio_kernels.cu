@@ -1416,21 +1416,33 @@ constexpr int kWindowThreadsMax = kWindowThreads;
 // drain loses to its spills; FP64: 384 117.0, 480 128.5.
 constexpr int kZhsThreadsFloat = 768;
 constexpr int kZhsThreadsDouble = 384;
-template <class Amp>
+// Two passes (fixed point): the track loop alone runs larger CTAs (FP32 768
+// threads, FP64 480: the most its 72-byte staging slots allow beside an
+// 8192-bin window), the drain pass 384.
+constexpr int kZhsLoopThreadsFloat = 768;
+constexpr int kZhsLoopThreadsDouble = 480;
+constexpr int kZhsDrainThreads = 384;
+// kPass: 0 one pass, 1 the track loop of two, 2 the drain pass of two.
+template <class Amp, int kPass = 0>
 constexpr int zhs_threads_max() {
-  return sizeof(Amp) == sizeof(float) ? kZhsThreadsFloat : kZhsThreadsDouble;
+  return kPass == 2   ? kZhsDrainThreads
+         : kPass == 1 ? (sizeof(Amp) == sizeof(float) ? kZhsLoopThreadsFloat : kZhsLoopThreadsDouble)
+                      : (sizeof(Amp) == sizeof(float) ? kZhsThreadsFloat : kZhsThreadsDouble);
 }
 // The ZHS block for a team of `threads`: the team when it is smaller than the
-// default team, else the largest block of the amplitude type.
-template <class Amp>
+// default team, else the largest block of the amplitude type and pass.
+template <class Amp, int kPass = 0>
 constexpr int zhs_block(int threads) {
-  return threads < kWindowThreads ? (threads < zhs_threads_max<Amp>() ? threads : zhs_threads_max<Amp>())
-                                  : zhs_threads_max<Amp>();
+  return threads < kWindowThreads
+             ? (threads < zhs_threads_max<Amp, kPass>() ? threads : zhs_threads_max<Amp, kPass>())
+             : zhs_threads_max<Amp, kPass>();
 }
-// staging slots of the ZHS kernel: 32 per warp
+// staging slots of the ZHS kernel: 32 per warp of its largest CTA
 template <class Amp>
 constexpr size_t staging_bytes() {
-  return static_cast<size_t>(zhs_threads_max<Amp>()) * sizeof(StagedSegment<Amp>);
+  int const a = zhs_threads_max<Amp, 0>(), b = zhs_threads_max<Amp, 1>(), c = zhs_threads_max<Amp, 2>();
+  int const most = a > b ? (a > c ? a : c) : (b > c ? b : c);
+  return static_cast<size_t>(most) * sizeof(StagedSegment<Amp>);
 }
 constexpr size_t kStagingBytes =
     staging_bytes<float>() > staging_bytes<double>() ? staging_bytes<float>() : staging_bytes<double>();
@@ -1597,16 +1609,30 @@ __device__ __forceinline__ void load_source_terms(const double* __restrict__ bas
   }
 }
 
-template <bool kFixed, class Amp, int kAlgorithm, bool kPre>
-__global__ void __launch_bounds__(kAlgorithm == 1 ? zhs_threads_max<Amp>() : kWindowThreadsMax, 1)
+// kPass 0: one pass over every item.  Two passes (fixed-point ZHS):
+// kPass 1 runs the track loop alone with unchecked window adds, appends the
+// deferred pairs of all its items to its CTA's list, flushes each item whose
+// window bound holds and records where its deferred pairs are; an item whose
+// bound does not hold, whose trace is longer than the window or whose pairs
+// do not fit in the list is handed back unflushed.  kPass 2 drains each
+// recorded item's pairs into a fresh window and projects the handed-back
+// items in full, as kPass 0 does.  The drain needs more registers than the
+// track loop (168 against 112 FP32, 135 FP64), so apart the track loop runs
+// without spills in larger CTAs.
+template <bool kFixed, class Amp, int kAlgorithm, bool kPre, int kPass = 0>
+__global__ void __launch_bounds__(kAlgorithm == 1 ? zhs_threads_max<Amp, kPass>() : kWindowThreadsMax, 1)
     windowed_kernel(const __grid_constant__ WorkPlan plan) {
+  static_assert(kPass == 0 || (kFixed && kAlgorithm == 1), "two passes: fixed-point ZHS");
   extern __shared__ __align__(16) unsigned long long window[];
   __shared__ unsigned long long item_shared;
   __shared__ ObserverCache observer;
   __shared__ float window_bound;
   __shared__ unsigned deferred_total;
-  // ZHS: this CTA's list of the deferred pairs of its current item
-  unsigned* const deferred_list = plan.deferred + static_cast<size_t>(blockIdx.x) * plan.deferred_stride;
+  // this CTA's list of the deferred pairs of its current item (kPass 1: of
+  // all its items, from `used` on; kPass 2: of the items it projects in full)
+  unsigned* const deferred_list = (kPass == 2 ? plan.drain_deferred : plan.deferred) +
+                                  static_cast<size_t>(blockIdx.x) * plan.deferred_stride;
+  uint32_t used = 0;  // kPass 1: entries of the list taken by earlier items
   Counts c;
   for (;;) {
     __syncthreads();
@@ -1623,12 +1649,25 @@ __global__ void __launch_bounds__(kAlgorithm == 1 ? zhs_threads_max<Amp>() : kWi
     uint64_t const valid = *ev.valid_tracks;
     uint64_t const track_count = valid < ev.last_track ? valid : ev.last_track;
     uint64_t const begin = ev.first_track + slice_chunk * ev.chunk_size;
-    if (begin >= track_count) continue;
+    ItemState state{blockIdx.x, used, 0u, 0u};
+    if constexpr (kPass == 2) {
+      state = plan.item_state[item];
+      if (!state.redo && state.count == 0u) continue;  // done by the first pass
+    }
+    bool const drain_only = kPass == 2 && !state.redo;
+    if (begin >= track_count) {
+      if (kPass == 1 && threadIdx.x == 0) plan.item_state[item] = state;
+      continue;
+    }
     uint64_t const end = begin + ev.chunk_size < track_count ? begin + ev.chunk_size : track_count;
-    if (threadIdx.x == 0) observer = ev.observers[algorithm][oi];
-    ObserverCache const& o = observer;
     uint64_t const bins = ev.observers[algorithm][oi].bins;
     uint32_t const width = static_cast<uint32_t>(bins < ev.window ? bins : ev.window);
+    if (kPass == 1 && bins > width) {  // checked adds past the window: the second pass
+      if (threadIdx.x == 0) plan.item_state[item] = ItemState{blockIdx.x, used, 0u, 1u};
+      continue;
+    }
+    if (threadIdx.x == 0) observer = ev.observers[algorithm][oi];
+    ObserverCache const& o = observer;
 
     // zero the window (3 rows of width bins); the barrier also publishes `observer`
     for (uint32_t j = threadIdx.x; j < 3 * width; j += blockDim.x) window[j] = 0ull;
@@ -1657,6 +1696,8 @@ __global__ void __launch_bounds__(kAlgorithm == 1 ? zhs_threads_max<Amp>() : kWi
         (threadIdx.x >> 5) * 32u;
     unsigned const lane = threadIdx.x & 31u;
     Counts const saved = c;
+    bool redo = false;  // kPass 1: the item goes back to the second pass
+    unsigned n = 0;     // deferred pairs of the item
     // Fixed point, whole trace in the window: the window takes unchecked
     // adds, and `c.mag` bounds the sum of |increments| of this thread.  If the
     // block's bound stays below 2^61, no partial sum of any bin can have left
@@ -1677,7 +1718,7 @@ __global__ void __launch_bounds__(kAlgorithm == 1 ? zhs_threads_max<Amp>() : kWi
       c.mag = 0.f;
       if (threadIdx.x == 0) deferred_total = 0u;
       __syncthreads();
-      for (uint64_t base = begin; base < end; base += blockDim.x) {
+      for (uint64_t base = begin; !drain_only && base < end; base += blockDim.x) {
         uint64_t const i = base + threadIdx.x;
         bool deferred = false;
         unsigned hint = 0u;  // CoREAS: the near-Cherenkov decision, in the list entry's top bits
@@ -1706,7 +1747,7 @@ __global__ void __launch_bounds__(kAlgorithm == 1 ? zhs_threads_max<Amp>() : kWi
             }
             deposit_unchecked(staging, seg, o, sink);
           } else {
-            deposit_staged<kFixed>(staging, seg, o, sink, c);
+            if constexpr (kPass != 1) deposit_staged<kFixed>(staging, seg, o, sink, c);
           }
         }
         unsigned const ballot = __ballot_sync(0xffffffffu, deferred);
@@ -1715,19 +1756,32 @@ __global__ void __launch_bounds__(kAlgorithm == 1 ? zhs_threads_max<Amp>() : kWi
           unsigned slot = 0;
           if (lane == 0) slot = atomicAdd(&deferred_total, static_cast<unsigned>(__popc(ballot)));
           slot = __shfl_sync(0xffffffffu, slot, 0);
-          if (deferred) deferred_list[slot + rank] = static_cast<unsigned>(i - begin) | hint;
+          uint64_t const at = static_cast<uint64_t>(used) + slot + rank;  // used: 0 but in kPass 1
+          if (deferred && (kPass != 1 || at < plan.deferred_stride))
+            deferred_list[at] = static_cast<unsigned>(i - begin) | hint;
         }
       }
       __syncthreads();
-      unsigned const n = deferred_total;  // at most end - begin <= deferred_stride
-      for (unsigned from = (threadIdx.x >> 5) * 32u; from < n; from += (blockDim.x >> 5) * 32u) {
+      // at most end - begin <= deferred_stride (kPass 1: over the list's end
+      // when used + n is)
+      n = drain_only ? state.count : deferred_total;
+      if (kPass == 1 && static_cast<uint64_t>(used) + n > plan.deferred_stride) {
+        redo = true;
+        break;
+      }
+      unsigned const* const list =
+          drain_only ? plan.deferred + static_cast<size_t>(state.cta) * plan.deferred_stride + state.begin
+                     : deferred_list;
+      for (unsigned from = (threadIdx.x >> 5) * 32u; kPass != 1 && from < n; from += (blockDim.x >> 5) * 32u) {
         unsigned const count = n - from < 32u ? n - from : 32u;
         Counts d;
-        if (kAlgorithm == 1) {
-          d = zhs_drain<kFixed, kFilter, Amp>(ev.tracks, begin, deferred_list + from, count,
+        if constexpr (kAlgorithm == 1 && kPass == 1) {
+          (void)count;
+        } else if (kAlgorithm == 1) {
+          d = zhs_drain<kFixed, kFilter, Amp>(ev.tracks, begin, list + from, count,
                                               ev.propagation, o, sink, staging);
         } else if (lane < count) {
-          unsigned const entry = deferred_list[from + lane];
+          unsigned const entry = list[from + lane];
           d = coreas_drain_pair<kFixed, Amp, kPre>(ev.tracks, begin + (entry & kDeferredOffsetMask),
                                                    entry >> kDeferredHintShift, ev.propagation, o, sink);
         }
@@ -1749,8 +1803,21 @@ __global__ void __launch_bounds__(kAlgorithm == 1 ? zhs_threads_max<Amp>() : kWi
       float const block_bound = window_bound;
       __syncthreads();
       if (block_bound < 0x1p61f) break;
+      if (kPass == 1) {
+        redo = true;
+        break;
+      }
       if (threadIdx.x == 0 && plan.reruns) atomicAdd(plan.reruns, 1ull);
       c = saved;
+    }
+    if constexpr (kPass == 1) {
+      if (redo) {  // unflushed: the second pass projects the item in full
+        c = saved;
+        if (threadIdx.x == 0) plan.item_state[item] = ItemState{blockIdx.x, used, 0u, 1u};
+        continue;
+      }
+      if (threadIdx.x == 0) plan.item_state[item] = ItemState{blockIdx.x, used, n, 0u};
+      used += n;
     }
 
     // flush: non-zero bins, checked global adds
@@ -1877,16 +1944,29 @@ bool plan_precomputed(WorkPlan const& plan) {
   return true;
 }
 
-template <bool kFixed, class Amp, int kAlgorithm, bool kPre>
+template <bool kFixed, class Amp, int kAlgorithm, bool kPre, int kPass = 0>
 cudaError_t windowed_launch(WorkPlan const& plan, int ctas, int threads, cudaStream_t stream) {
   size_t const bytes = windowed_smem_bytes<Amp>(plan.window, kAlgorithm);
-  cudaError_t err = cudaFuncSetAttribute(windowed_kernel<kFixed, Amp, kAlgorithm, kPre>,
+  cudaError_t err = cudaFuncSetAttribute(windowed_kernel<kFixed, Amp, kAlgorithm, kPre, kPass>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(bytes));
   if (err != cudaSuccess) return err;
-  int const block = kAlgorithm == 1 ? zhs_block<Amp>(threads) : threads;
-  windowed_kernel<kFixed, Amp, kAlgorithm, kPre><<<ctas, block, bytes, stream>>>(plan);
+  int const block = kAlgorithm == 1 ? zhs_block<Amp, kPass>(threads) : threads;
+  windowed_kernel<kFixed, Amp, kAlgorithm, kPre, kPass><<<ctas, block, bytes, stream>>>(plan);
   return cudaGetLastError();
+}
+
+// The two passes of a fixed-point ZHS launch, one after the other on the
+// stream; the second draws items from its own counter.
+template <class Amp, bool kPre>
+cudaError_t windowed_two_pass(WorkPlan const& plan, int ctas, int threads, cudaStream_t stream) {
+  cudaError_t err = windowed_launch<true, Amp, 1, kPre, 1>(plan, ctas, threads, stream);
+  if (err != cudaSuccess) return err;
+  err = cudaMemsetAsync(plan.drain_next_item, 0, sizeof(unsigned), stream);
+  if (err != cudaSuccess) return err;
+  WorkPlan second = plan;
+  second.next_item = plan.drain_next_item;
+  return windowed_launch<true, Amp, 1, kPre, 2>(second, ctas, threads, stream);
 }
 
 template <bool kFixed, class Amp, int kAlgorithm>
@@ -1894,8 +1974,18 @@ cudaError_t windowed_dispatch_algorithm(WorkPlan const& plan, int ctas, int thre
                                         cudaStream_t stream) {
   if (plan.deferred == nullptr || plan.deferred_stride < deferred_list_stride(plan))
     return cudaErrorInvalidValue;
-  return plan_precomputed(plan) ? windowed_launch<kFixed, Amp, kAlgorithm, true>(plan, ctas, threads, stream)
-                                : windowed_launch<kFixed, Amp, kAlgorithm, false>(plan, ctas, threads, stream);
+  bool const pre = plan_precomputed(plan);
+  if (plan.item_state != nullptr) {
+    if constexpr (kFixed && kAlgorithm == 1) {
+      if (plan.drain_deferred == nullptr || plan.drain_next_item == nullptr) return cudaErrorInvalidValue;
+      return pre ? windowed_two_pass<Amp, true>(plan, ctas, threads, stream)
+                 : windowed_two_pass<Amp, false>(plan, ctas, threads, stream);
+    } else {
+      return cudaErrorInvalidValue;
+    }
+  }
+  return pre ? windowed_launch<kFixed, Amp, kAlgorithm, true>(plan, ctas, threads, stream)
+             : windowed_launch<kFixed, Amp, kAlgorithm, false>(plan, ctas, threads, stream);
 }
 
 template <bool kFixed, class Amp>
@@ -1920,6 +2010,12 @@ int ctas_per_sm(int window, int threads) {
   probe(windowed_kernel<kFixed, Amp, 0, true>, threads, 0);
   probe(windowed_kernel<kFixed, Amp, 1, false>, zhs_block<Amp>(threads), 1);
   probe(windowed_kernel<kFixed, Amp, 1, true>, zhs_block<Amp>(threads), 1);
+  if constexpr (kFixed) {  // the two passes
+    probe(windowed_kernel<true, Amp, 1, false, 1>, zhs_block<Amp, 1>(threads), 1);
+    probe(windowed_kernel<true, Amp, 1, true, 1>, zhs_block<Amp, 1>(threads), 1);
+    probe(windowed_kernel<true, Amp, 1, false, 2>, zhs_block<Amp, 2>(threads), 1);
+    probe(windowed_kernel<true, Amp, 1, true, 2>, zhs_block<Amp, 2>(threads), 1);
+  }
   return worst;
 }
 

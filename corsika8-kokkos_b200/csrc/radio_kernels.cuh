@@ -82,6 +82,15 @@ bool shared_destination(ObserverCache const* observers, std::size_t count, Desti
 constexpr int kMaxEventsPerLaunch = 64;
 constexpr int kPlanEntries = kMaxEventsPerLaunch + 1;  // + the short-chunk tail of the last event
 constexpr int kWindowThreads = 640;  // upper bound (and default) of the windowed block size
+// Where the first pass of a two-pass ZHS launch left a work item's deferred
+// pairs: `count` entries from `begin` of CTA `cta`'s list; `redo` when the
+// second pass projects the item in full (its window could not be shown free
+// of overflow, its trace was longer than the window, or the CTA's list was
+// full).
+struct ItemState {
+  uint32_t cta, begin, count, redo;
+};
+
 struct WorkPlan {
   EventPlan events[kPlanEntries];
   int32_t algorithm;        // 0: CoREAS items, 1: ZHS items
@@ -97,6 +106,16 @@ struct WorkPlan {
   // Items run again with checked window adds (the unchecked run's bound did
   // not hold); counted when not null.
   unsigned long long* reruns;
+  // Two-pass ZHS (fixed point), when item_state is set: the first pass runs
+  // the track loop alone and keeps each CTA's deferred pairs of all its items
+  // in its list (`deferred`), the second drains them item by item and
+  // projects in full the items the first handed back, with its own lists
+  // (`drain_deferred`, deferred_stride entries a CTA) and work counter.
+  // The drain needs more registers than the track loop, so the track loop
+  // runs larger CTAs on its own (attach_deferred sets these).
+  ItemState* item_state;
+  unsigned int* drain_deferred;
+  unsigned int* drain_next_item;
 };
 
 // A work item spans at most kMaxChunkTracks tracks: a deferred-list entry is
@@ -112,6 +131,31 @@ inline uint32_t deferred_list_stride(WorkPlan const& plan) {
   for (uint32_t e = 0; e < plan.event_count; ++e)
     if (plan.events[e].chunk_size > stride) stride = plan.events[e].chunk_size;
   return stride;
+}
+
+// ZHS launches in fixed point run in two passes.
+inline bool two_pass(WorkPlan const& plan, bool fixed) { return fixed && plan.algorithm == 1; }
+
+// 32-bit words of deferred-list storage a launch of `plan` (deferred_stride
+// and total_items set) over `ctas` CTAs needs: its CTAs' lists, and for two
+// passes the second pass's lists, the items' states and its work counter.
+inline uint64_t deferred_words(WorkPlan const& plan, uint64_t ctas, bool fixed) {
+  uint64_t const lists = ctas * plan.deferred_stride;
+  if (!two_pass(plan, fixed)) return lists;
+  return 2 * lists + plan.total_items * (sizeof(ItemState) / sizeof(unsigned)) + 1;
+}
+
+// Points the plan's deferred-list storage into `words` (deferred_words of it).
+inline void attach_deferred(WorkPlan& plan, unsigned* words, uint64_t ctas, bool fixed) {
+  uint64_t const lists = ctas * plan.deferred_stride;
+  plan.deferred = words;
+  plan.item_state = nullptr;
+  plan.drain_deferred = nullptr;
+  plan.drain_next_item = nullptr;
+  if (!two_pass(plan, fixed)) return;
+  plan.drain_deferred = words + lists;
+  plan.item_state = reinterpret_cast<ItemState*>(words + 2 * lists);
+  plan.drain_next_item = words + 2 * lists + plan.total_items * (sizeof(ItemState) / sizeof(unsigned));
 }
 
 // Appends the (chunk, observer) work items of `ev` for plan.algorithm to

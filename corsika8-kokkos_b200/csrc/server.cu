@@ -766,7 +766,7 @@ class Server {
         uint64_t const items = plan.total_items;
         if (ctas > items) ctas = items;
         plan.deferred_stride = deferred_list_stride(plan);
-        plan.deferred = deferred_lists(ctas * plan.deferred_stride);
+        attach_deferred(plan, deferred_lists(deferred_words(plan, ctas, fixed)), ctas, fixed);
         check(cudaMemsetAsync(counter, 0, sizeof(unsigned), compute_), "server work counter");
         check(launch_windowed(plan, fixed, precision, static_cast<int>(ctas), threads_, compute_),
               "server windowed launch");
