@@ -147,8 +147,8 @@ typedef struct c8r_config {
 /* corsika/kokkos/runtime/TuningParameters.hpp:14-21; zero keeps defaults.
  * track_tile_size = tracks per windowed CTA chunk, observer_tile_size = bins
  * per shared-memory window, team_size = threads per CoREAS CTA (a team below
- * the default 640 also caps the ZHS CTA, which otherwise runs 768 threads with
- * FP32 amplitudes and 384 with FP64). */
+ * the default 640 also caps the ZHS CTAs, which otherwise take the largest
+ * block of their pass and amplitude type: 384 to 768 threads). */
 typedef struct c8r_tuning {
   uint64_t batch_size;
   uint64_t chunk_size;
@@ -507,7 +507,7 @@ typedef struct c8r_server_options {
   uint64_t block_tracks; /* tracks per kinematics block; 0 = 1048576 */
   uint64_t chunk_tracks; /* tracks per work item; 0 = 131072 (divides block_tracks, at most 2^30) */
   uint64_t round_pairs;  /* track-observer pairs per round; 0 = 1e9 */
-  uint32_t team_size;    /* threads per windowed CTA; 0 = 640 (ZHS: 768 FP32, 384 FP64) */
+  uint32_t team_size;    /* threads per windowed CTA; 0 = 640 (ZHS CTAs: 384 to 768) */
   uint32_t reserved_[7];
 } c8r_server_options;
 typedef struct c8r_server_event_info {
