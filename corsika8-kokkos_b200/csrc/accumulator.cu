@@ -941,7 +941,9 @@ class Accumulator {
     if (lists.count < entries) {
       check(cudaStreamSynchronize(stream_), "deferred list fence");
       DeviceBuffer<unsigned> fresh;
-      fresh.allocate(entries);
+      // a quarter more than asked: launch sizes vary, and each growth
+      // synchronises the device
+      fresh.allocate(entries + entries / 4);
       lists.swap(fresh);
       stats_.device_bytes = device_bytes();
     }
@@ -1300,10 +1302,20 @@ class Batch {
         l.threads = threads;
         uint64_t ctas = static_cast<uint64_t>(per_sm) * sms;
         // the events of this launch; the last one ends the work list on short items
+        // at most kMaxEventsPerLaunch events and, for two-pass (fixed-point
+        // ZHS) launches, past the first event kMaxPairsPerLaunch pairs: their
+        // first pass's lists grow with the launch's pairs
         std::vector<std::size_t> members;
         std::size_t j = first;
-        for (; j < active.size() && members.size() < static_cast<std::size_t>(kMaxEventsPerLaunch); ++j)
-          if (active[j].second.observer_count[algorithm] != 0) members.push_back(j);
+        uint64_t pairs = 0;
+        for (; j < active.size() && members.size() < static_cast<std::size_t>(kMaxEventsPerLaunch); ++j) {
+          EventPlan const& e = active[j].second;
+          if (e.observer_count[algorithm] == 0) continue;
+          uint64_t const p = static_cast<uint64_t>(e.chunks) * e.chunk_size * e.observer_count[algorithm];
+          if (algorithm == 1 && fixed && !members.empty() && pairs + p > kMaxPairsPerLaunch) break;
+          members.push_back(j);
+          pairs += p;
+        }
         first = j;
         if (members.empty()) continue;
         for (std::size_t m = 0; m < members.size(); ++m)
@@ -1348,7 +1360,7 @@ class Batch {
       }
       graphs_.clear();
       DeviceBuffer<unsigned> fresh;
-      fresh.allocate(entries);
+      fresh.allocate(entries + entries / 4);  // a quarter more: each growth synchronises
       deferred_.swap(fresh);
     }
     return deferred_.ptr;

@@ -1630,8 +1630,10 @@ __global__ void __launch_bounds__(kAlgorithm == 1 ? zhs_threads_max<Amp, kPass>(
   __shared__ unsigned deferred_total;
   // this CTA's list of the deferred pairs of its current item (kPass 1: of
   // all its items, from `used` on; kPass 2: of the items it projects in full)
-  unsigned* const deferred_list = (kPass == 2 ? plan.drain_deferred : plan.deferred) +
-                                  static_cast<size_t>(blockIdx.x) * plan.deferred_stride;
+  unsigned* const deferred_list =
+      kPass == 2 ? plan.drain_deferred + static_cast<size_t>(blockIdx.x) * plan.deferred_stride
+      : kPass == 1 ? plan.deferred + static_cast<size_t>(blockIdx.x) * plan.deferred_capacity
+                   : plan.deferred + static_cast<size_t>(blockIdx.x) * plan.deferred_stride;
   uint32_t used = 0;  // kPass 1: entries of the list taken by earlier items
   Counts c;
   for (;;) {
@@ -1757,7 +1759,7 @@ __global__ void __launch_bounds__(kAlgorithm == 1 ? zhs_threads_max<Amp, kPass>(
           if (lane == 0) slot = atomicAdd(&deferred_total, static_cast<unsigned>(__popc(ballot)));
           slot = __shfl_sync(0xffffffffu, slot, 0);
           uint64_t const at = static_cast<uint64_t>(used) + slot + rank;  // used: 0 but in kPass 1
-          if (deferred && (kPass != 1 || at < plan.deferred_stride))
+          if (deferred && (kPass != 1 || at < plan.deferred_capacity))
             deferred_list[at] = static_cast<unsigned>(i - begin) | hint;
         }
       }
@@ -1765,12 +1767,12 @@ __global__ void __launch_bounds__(kAlgorithm == 1 ? zhs_threads_max<Amp, kPass>(
       // at most end - begin <= deferred_stride (kPass 1: over the list's end
       // when used + n is)
       n = drain_only ? state.count : deferred_total;
-      if (kPass == 1 && static_cast<uint64_t>(used) + n > plan.deferred_stride) {
+      if (kPass == 1 && static_cast<uint64_t>(used) + n > plan.deferred_capacity) {
         redo = true;
         break;
       }
       unsigned const* const list =
-          drain_only ? plan.deferred + static_cast<size_t>(state.cta) * plan.deferred_stride + state.begin
+          drain_only ? plan.deferred + static_cast<size_t>(state.cta) * plan.deferred_capacity + state.begin
                      : deferred_list;
       for (unsigned from = (threadIdx.x >> 5) * 32u; kPass != 1 && from < n; from += (blockDim.x >> 5) * 32u) {
         unsigned const count = n - from < 32u ? n - from : 32u;
@@ -1977,7 +1979,9 @@ cudaError_t windowed_dispatch_algorithm(WorkPlan const& plan, int ctas, int thre
   bool const pre = plan_precomputed(plan);
   if (plan.item_state != nullptr) {
     if constexpr (kFixed && kAlgorithm == 1) {
-      if (plan.drain_deferred == nullptr || plan.drain_next_item == nullptr) return cudaErrorInvalidValue;
+      if (plan.drain_deferred == nullptr || plan.drain_next_item == nullptr ||
+          plan.deferred_capacity < plan.deferred_stride)
+        return cudaErrorInvalidValue;
       return pre ? windowed_two_pass<Amp, true>(plan, ctas, threads, stream)
                  : windowed_two_pass<Amp, false>(plan, ctas, threads, stream);
     } else {

@@ -80,6 +80,9 @@ bool shared_destination(ObserverCache const* observers, std::size_t count, Desti
 // observer) items drawn from an atomic counter.  Passed as a __grid_constant__
 // kernel parameter (no host-to-device copy; graph-capturable).
 constexpr int kMaxEventsPerLaunch = 64;
+// Pairs a batched launch takes beyond its first event (its two-pass ZHS
+// storage stays near 8% of them).
+constexpr uint64_t kMaxPairsPerLaunch = 4000000000ull;
 constexpr int kPlanEntries = kMaxEventsPerLaunch + 1;  // + the short-chunk tail of the last event
 constexpr int kWindowThreads = 640;  // upper bound (and default) of the windowed block size
 // Where the first pass of a two-pass ZHS launch left a work item's deferred
@@ -112,10 +115,12 @@ struct WorkPlan {
   // projects in full the items the first handed back, with its own lists
   // (`drain_deferred`, deferred_stride entries a CTA) and work counter.
   // The drain needs more registers than the track loop, so the track loop
-  // runs larger CTAs on its own (attach_deferred sets these).
+  // runs larger CTAs on its own (attach_deferred sets these).  The first
+  // pass's lists hold `deferred_capacity` entries a CTA.
   ItemState* item_state;
   unsigned int* drain_deferred;
   unsigned int* drain_next_item;
+  uint32_t deferred_capacity;
 };
 
 // A work item spans at most kMaxChunkTracks tracks: a deferred-list entry is
@@ -133,29 +138,63 @@ inline uint32_t deferred_list_stride(WorkPlan const& plan) {
   return stride;
 }
 
-// ZHS launches in fixed point run in two passes.
-inline bool two_pass(WorkPlan const& plan, bool fixed) { return fixed && plan.algorithm == 1; }
+// Pairs a launch of `plan` covers at most (its items' chunks at full length).
+inline uint64_t plan_pairs(WorkPlan const& plan) {
+  uint64_t pairs = 0;
+  for (uint32_t e = 0; e < plan.event_count; ++e) {
+    EventPlan const& ev = plan.events[e];
+    pairs += static_cast<uint64_t>(ev.chunks) * ev.chunk_size * ev.observer_count[plan.algorithm];
+  }
+  return pairs;
+}
+
+// First-pass list entries a CTA of a two-pass launch holds: the deferred
+// pairs of all its items, sized for 8% of its share of the launch's pairs
+// (ZHS defers 3% on the 1e7 x 160 workload) and at least one chunk; an item
+// past the end is handed back to the second pass (correct, slower).
+constexpr double kTwoPassDeferredShare = 0.08;
+// Launches whose two-pass storage would pass 2^30 words (4 GiB) run one pass.
+constexpr uint64_t kTwoPassMaxWords = 1ull << 30;
+
+inline uint64_t pass1_capacity(WorkPlan const& plan, uint64_t ctas) {
+  uint64_t const share = static_cast<uint64_t>(kTwoPassDeferredShare * static_cast<double>(plan_pairs(plan)) /
+                                               static_cast<double>(ctas > 0 ? ctas : 1)) + 1;
+  uint64_t const capacity = share > plan.deferred_stride ? share : plan.deferred_stride;
+  return capacity < 0xffffffffull ? capacity : 0xffffffffull;
+}
+
+inline uint64_t two_pass_words(WorkPlan const& plan, uint64_t ctas) {
+  return ctas * pass1_capacity(plan, ctas) + ctas * plan.deferred_stride +
+         plan.total_items * (sizeof(ItemState) / sizeof(unsigned)) + 1;
+}
+
+// ZHS launches in fixed point run in two passes when their storage fits.
+inline bool two_pass(WorkPlan const& plan, uint64_t ctas, bool fixed) {
+  return fixed && plan.algorithm == 1 && two_pass_words(plan, ctas) <= kTwoPassMaxWords;
+}
 
 // 32-bit words of deferred-list storage a launch of `plan` (deferred_stride
 // and total_items set) over `ctas` CTAs needs: its CTAs' lists, and for two
-// passes the second pass's lists, the items' states and its work counter.
+// passes the first pass's longer lists, the second pass's lists, the items'
+// states and its work counter.
 inline uint64_t deferred_words(WorkPlan const& plan, uint64_t ctas, bool fixed) {
-  uint64_t const lists = ctas * plan.deferred_stride;
-  if (!two_pass(plan, fixed)) return lists;
-  return 2 * lists + plan.total_items * (sizeof(ItemState) / sizeof(unsigned)) + 1;
+  if (!two_pass(plan, ctas, fixed)) return ctas * plan.deferred_stride;
+  return two_pass_words(plan, ctas);
 }
 
 // Points the plan's deferred-list storage into `words` (deferred_words of it).
 inline void attach_deferred(WorkPlan& plan, unsigned* words, uint64_t ctas, bool fixed) {
-  uint64_t const lists = ctas * plan.deferred_stride;
   plan.deferred = words;
   plan.item_state = nullptr;
   plan.drain_deferred = nullptr;
   plan.drain_next_item = nullptr;
-  if (!two_pass(plan, fixed)) return;
-  plan.drain_deferred = words + lists;
-  plan.item_state = reinterpret_cast<ItemState*>(words + 2 * lists);
-  plan.drain_next_item = words + 2 * lists + plan.total_items * (sizeof(ItemState) / sizeof(unsigned));
+  plan.deferred_capacity = plan.deferred_stride;
+  if (!two_pass(plan, ctas, fixed)) return;
+  uint64_t const first = ctas * pass1_capacity(plan, ctas);
+  plan.deferred_capacity = static_cast<uint32_t>(pass1_capacity(plan, ctas));
+  plan.drain_deferred = words + first;
+  plan.item_state = reinterpret_cast<ItemState*>(words + first + ctas * plan.deferred_stride);
+  plan.drain_next_item = reinterpret_cast<unsigned*>(plan.item_state + plan.total_items);
 }
 
 // Appends the (chunk, observer) work items of `ev` for plan.algorithm to

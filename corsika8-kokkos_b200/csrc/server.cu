@@ -703,12 +703,15 @@ class Server {
   // Grown after the rounds in flight on compute_ when a launch needs more.
   unsigned* deferred_lists(uint64_t entries) {
     if (deferred_entries_ < entries) {
+      // twice what is asked: round sizes vary, and each growth synchronises
+      // the device (the producers' ingest included)
+      uint64_t const grown = std::max<uint64_t>(entries, 2 * deferred_entries_);
       check(cudaStreamSynchronize(compute_), "deferred list fence");
       if (deferred_) cudaFree(deferred_);
       deferred_ = nullptr;
       deferred_entries_ = 0;
-      check(cudaMalloc(&deferred_, entries * sizeof(unsigned)), "deferred lists");
-      deferred_entries_ = entries;
+      check(cudaMalloc(&deferred_, grown * sizeof(unsigned)), "deferred lists");
+      deferred_entries_ = grown;
     }
     return deferred_;
   }
