@@ -206,6 +206,7 @@ class Statistics(C.Structure):
         ("zhs_kernel_time_ms", C.c_double),
         ("counters", Counters),
         ("window_reruns", C.c_uint64),
+        ("window_handbacks", C.c_uint64),
     ]
 
 

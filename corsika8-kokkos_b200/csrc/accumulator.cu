@@ -215,7 +215,7 @@ class Accumulator {
     counters_.allocate(1);
     slot_.allocate(1);
     next_item_.allocate(2);  // one work counter per algorithm
-    reruns_.allocate(1);
+    reruns_.allocate(2);  // items re-run with checked adds, items handed to a drain pass
     staging_.allocate(host_batch_);
     for (auto& h : host_) h.allocate(host_batch_);
     for (auto& e : host_ready_) check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
@@ -258,7 +258,7 @@ class Accumulator {
         check(cudaMemsetAsync(float_traces_[a].ptr, 0, float_traces_[a].bytes(), stream_), "memset");
     }
     check(cudaMemsetAsync(counters_.ptr, 0, sizeof(DeviceCounters), stream_), "memset");
-    check(cudaMemsetAsync(reruns_.ptr, 0, sizeof(unsigned long long), stream_), "memset");
+    check(cudaMemsetAsync(reruns_.ptr, 0, 2 * sizeof(unsigned long long), stream_), "memset");
     clear_staged();
     check(cudaStreamSynchronize(stream_), "reset fence");
     resolve_timing();
@@ -1022,6 +1022,7 @@ class Accumulator {
       plan.window = ev.window;
       plan.next_item = next_item_.ptr + algorithm;
       plan.reruns = reruns_.ptr;
+      plan.handbacks = reruns_.ptr + 1;
       uint64_t ctas = static_cast<uint64_t>(per_sm) * sms_;
       append_work(plan, ev, ctas, true);
       if (ctas > plan.total_items) ctas = plan.total_items;
@@ -1056,6 +1057,9 @@ class Accumulator {
     check(cudaMemcpyAsync(&host, counters_.ptr, sizeof(host), cudaMemcpyDeviceToHost, stream_),
           "counter download");
     check(cudaMemcpyAsync(&stats_.window_reruns, reruns_.ptr, sizeof(unsigned long long),
+                          cudaMemcpyDeviceToHost, stream_),
+          "counter download");
+    check(cudaMemcpyAsync(&stats_.window_handbacks, reruns_.ptr + 1, sizeof(unsigned long long),
                           cudaMemcpyDeviceToHost, stream_),
           "counter download");
     check(cudaStreamSynchronize(stream_), "counter fence");
@@ -1103,7 +1107,7 @@ class Accumulator {
   DeviceBuffer<DeviceCounters> counters_;
   DeviceBuffer<unsigned long long> slot_;
   DeviceBuffer<unsigned> next_item_;
-  DeviceBuffer<unsigned long long> reruns_;  // windowed items re-run with checked adds
+  DeviceBuffer<unsigned long long> reruns_;  // windowed items re-run with checked adds, handed back
   DeviceBuffer<unsigned> deferred_[2];  // per-CTA deferred-pair lists, by algorithm
   DeviceBuffer<double> tracks_;
   std::size_t capacity_ = 0;

@@ -1665,7 +1665,10 @@ __global__ void __launch_bounds__(kAlgorithm == 1 ? zhs_threads_max<Amp, kPass>(
     uint64_t const bins = ev.observers[algorithm][oi].bins;
     uint32_t const width = static_cast<uint32_t>(bins < ev.window ? bins : ev.window);
     if (kPass == 1 && bins > width) {  // checked adds past the window: the second pass
-      if (threadIdx.x == 0) plan.item_state[item] = ItemState{blockIdx.x, used, 0u, 1u};
+      if (threadIdx.x == 0) {
+        plan.item_state[item] = ItemState{blockIdx.x, used, 0u, 1u};
+        if (plan.handbacks) atomicAdd(plan.handbacks, 1ull);
+      }
       continue;
     }
     if (threadIdx.x == 0) observer = ev.observers[algorithm][oi];
@@ -1815,7 +1818,10 @@ __global__ void __launch_bounds__(kAlgorithm == 1 ? zhs_threads_max<Amp, kPass>(
     if constexpr (kPass == 1) {
       if (redo) {  // unflushed: the second pass projects the item in full
         c = saved;
-        if (threadIdx.x == 0) plan.item_state[item] = ItemState{blockIdx.x, used, 0u, 1u};
+        if (threadIdx.x == 0) {
+          plan.item_state[item] = ItemState{blockIdx.x, used, 0u, 1u};
+          if (plan.handbacks) atomicAdd(plan.handbacks, 1ull);
+        }
         continue;
       }
       if (threadIdx.x == 0) plan.item_state[item] = ItemState{blockIdx.x, used, n, 0u};

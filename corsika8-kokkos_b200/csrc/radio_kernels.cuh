@@ -109,6 +109,8 @@ struct WorkPlan {
   // Items run again with checked window adds (the unchecked run's bound did
   // not hold); counted when not null.
   unsigned long long* reruns;
+  // Items the first pass of two handed to the second; counted when not null.
+  unsigned long long* handbacks;
   // Two-pass ZHS (fixed point), when item_state is set: the first pass runs
   // the track loop alone and keeps each CTA's deferred pairs of all its items
   // in its list (`deferred`), the second drains them item by item and

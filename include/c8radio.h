@@ -213,6 +213,10 @@ typedef struct c8r_statistics {
   uint64_t window_reruns;     /* windowed work items projected again with checked adds
                                  (their unchecked run could not exclude an overflow);
                                  read with the counters at download */
+  uint64_t window_handbacks;  /* ZHS work items the track-loop pass of a two-pass launch
+                                 handed to the drain pass to project in full (trace past
+                                 the window, window bound not shown, or its deferred
+                                 pairs past its CTA's list); read at download */
 } c8r_statistics;
 
 /* Measured device rates used as roofline denominators (c8r_probe_peaks). */

@@ -417,6 +417,36 @@ def test_window_cap_on_adds_per_thread(pkg, oracle, showers, torch_cuda):
 
 
 @pytest.mark.parametrize("precision", [0, 1])
+def test_two_pass_handback_when_the_lists_fill(pkg, oracle, showers, torch_cuda, precision):
+    """Fixed-point ZHS runs the track loop and the drain as two passes.  With
+    subtrack refinement 2 every ZHS pair is deferred, and with 256-track work
+    items each CTA's first-pass list (one item's length here) is full after
+    its first item: every later item is handed back unflushed and projected
+    in full by the second pass.  The traces equal the oracle's (FP64: bit for
+    bit; mixed: counters equal, traces within 1e-4), so no pair is lost or
+    deposited twice."""
+    wl, records = _workload_records(showers, "plain_c0", 20_000, seed=41)
+    config = showers.make_config(wl, precision=precision, kernel=2)
+    config.zhs_subtrack_refinement = 2
+    got = gpu_project(pkg, torch_cuda, config, records, tuning=pkg.TuningParameters(track_tile_size=256))
+    exact = showers.make_config(wl)
+    exact.zhs_subtrack_refinement = 2
+    want = oracle.restatement().project(exact, records, threads=16)
+    assert got[3].window_handbacks > 0
+    if precision == 0:
+        assert_same(got[:3], want, True)
+    else:
+        for key in EXACT_COUNTERS:
+            assert got[2][key] == want[2][key], key
+        scale = exact.fixed_point_field_limit_v_per_m / 2.0 ** 62
+        fs = wl["observers"]["sample_rate_hz"][0]
+        for a, factor in ((0, 1.0), (1, fs)):
+            err = relative_l2_per_trace(got[a] * (scale / factor), want[a] * (scale / factor),
+                                        wl["observers"])
+            assert err.max() <= 1e-4, (a, err.max())
+
+
+@pytest.mark.parametrize("precision", [0, 1])
 def test_traces_longer_than_the_window(pkg, oracle, showers, torch_cuda, precision):
     """20000-bin traces exceed the largest shared-memory window: the bins past
     it go to checked global atomics, and such items never take unchecked window
