@@ -62,6 +62,8 @@ def parse_args():
     p.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
     p.add_argument("--kernel", choices=["windowed", "direct"], default="windowed")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--e2e-batch", type=int, default=1 << 22,
+                   help="host batch (records) of the end-to-end leg")
     p.add_argument("--no-baseline", action="store_true")
     p.add_argument("--no-variants", action="store_true",
                    help="skip the FP64 windowed and plain FP64 direct comparison runs")
@@ -814,11 +816,11 @@ def run_e2e(pkg, showers, wl, records, precision, kernel, stream, args, torch, b
     The library uploads the span of each record the ingest reads (208 of 752
     bytes) with a pitched copy.
 
-    Host batches of 2^21 records (1.5 GB): each copy hides behind the previous
-    batch's projection; the library starts at an eighth of that and grows each
-    batch by a quarter, so the first projection waits for a short copy only."""
+    Host batches of up to 2^22 records (--e2e-batch): each copy hides behind
+    the previous batch's projection; the library starts at 1/32 of that and
+    doubles each batch, so the first projection waits for a short copy only."""
     config = showers.make_config(wl, precision=precision, kernel=kernel)
-    tuning = pkg.TuningParameters(batch_size=1 << 21)
+    tuning = pkg.TuningParameters(batch_size=args.e2e_batch)
     acc = pkg.RadioAccumulator(config, tuning, stream=stream.cuda_stream)
     cudart = torch.cuda.cudart()
     registered = cudart.cudaHostRegister(records.ctypes.data, records.nbytes, 0) == 0
