@@ -190,7 +190,7 @@ def test_host_enqueue_batches_match_device_path(pkg, oracle, showers, torch_cuda
 def test_short_tail_items_and_ramped_pinned_batches(pkg, oracle, showers, torch_cuda):
     """Work lists that end on quarter-size chunks (the last large chunk split in
     four) and pinned host input copied straight from the caller's memory in
-    batches growing from an eighth of the host batch by a quarter each (the
+    batches doubling from 1/32 of the host batch (at least 8192 records; the
     last one partial) give the traces of one plain device launch."""
     wl, records = _workload_records(showers, "tiled_c1", 100_000, seed=41)
     want = oracle.restatement().project(showers.make_config(wl), records, threads=16)
@@ -213,20 +213,20 @@ def test_short_tail_items_and_ramped_pinned_batches(pkg, oracle, showers, torch_
         stats = acc.statistics()
         acc.close()
         assert_same(got, plain, True)
-        # batches of 8192, then each a quarter longer (up to 65536), the last one partial
+        # batches of 8192, then each twice as long (up to 65536), the last one partial
         sizes, size, left = [], 8192, records.size
         while left:
             sizes.append(min(size, left))
             left -= sizes[-1]
-            size = min(65536, size + size // 4)
-        assert stats.host_track_batches == len(sizes) == 7
+            size = min(65536, 2 * size)
+        assert stats.host_track_batches == len(sizes) == 4
         assert stats.host_tracks_enqueued == records.size
 
 
 def test_growing_host_batches_grow_the_deferred_lists(pkg, oracle, showers, torch_cuda):
-    """Pinned host batches that grow (automatic chunks from 8192 to 10000 tracks)
-    make the accumulator grow its per-CTA deferred-pair lists between launches;
-    the traces equal the oracle's."""
+    """Pinned host batches that grow (8192 to 131072 records; automatic chunks
+    from 8192 to 16384 tracks) make the accumulator grow its per-CTA
+    deferred-pair lists between launches; the traces equal the oracle's."""
     wl, records = _workload_records(showers, "plain_c0", 300_000, seed=43)
     pinned = torch_cuda.empty(records.nbytes, dtype=torch_cuda.uint8, pin_memory=True).numpy()
     pinned[:] = records.view(np.uint8)
