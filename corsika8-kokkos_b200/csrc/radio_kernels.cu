@@ -865,7 +865,13 @@ __device__ __forceinline__ void deposit_unchecked(StagedSegment<Amp>* staging, S
   ObserverCache grid;  // the converting fields in registers
   grid.fixed_scale = o.fixed_scale;
   grid.fixed_scale_f = o.fixed_scale_f;
-  unsigned long long* const win = sink.win;
+  // The adds go through a generic pointer: where the compiler can tell the
+  // window is shared memory it emits shared-space 64-bit atomics, which this
+  // GPU executes as about one instruction per active lane (the ZHS track
+  // loop alone, one pass of two, ran at twice the atomic wavefronts of the
+  // single-pass kernel's generic adds on the same samples).
+  unsigned long long* win = sink.win;
+  asm volatile("" : "+l"(win));
   uint32_t const width = sink.width;
   // kPer bins per lane per step, their owner searches interleaved
   constexpr int kPer = sizeof(Amp) == sizeof(float) ? 2 : 4;  // measured best of 2 and 4
@@ -1422,7 +1428,8 @@ constexpr int kZhsThreadsDouble = 384;
 constexpr int kZhsLoopThreadsFloat = 768;
 constexpr int kZhsLoopThreadsDouble = 480;
 constexpr int kZhsDrainThreads = 384;
-// kPass: 0 one pass, 1 the track loop of two, 2 the drain pass of two.
+// kPass: 0 one pass; of a two-pass launch 1 the track loop, 2 the drain, 3
+// the handed-back items in full (as one pass).
 template <class Amp, int kPass = 0>
 constexpr int zhs_threads_max() {
   return kPass == 2   ? kZhsDrainThreads
@@ -1614,11 +1621,12 @@ __device__ __forceinline__ void load_source_terms(const double* __restrict__ bas
 // deferred pairs of all its items to its CTA's list, flushes each item whose
 // window bound holds and records where its deferred pairs are; an item whose
 // bound does not hold, whose trace is longer than the window or whose pairs
-// do not fit in the list is handed back unflushed.  kPass 2 drains each
-// recorded item's pairs into a fresh window and projects the handed-back
-// items in full, as kPass 0 does.  The drain needs more registers than the
-// track loop (168 against 112 FP32, 135 FP64), so apart the track loop runs
-// without spills in larger CTAs.
+// do not fit in the list is handed back unflushed, and once its list has
+// overflowed a CTA hands back its later items unprojected.  kPass 2 drains
+// each recorded item's pairs into a fresh window; kPass 3 projects the
+// handed-back items in full, as kPass 0 does.  The drain needs more
+// registers than the track loop (168 against 80 FP32, 118 FP64), so apart
+// the track loop runs without spills in larger CTAs.
 template <bool kFixed, class Amp, int kAlgorithm, bool kPre, int kPass = 0>
 __global__ void __launch_bounds__(kAlgorithm == 1 ? zhs_threads_max<Amp, kPass>() : kWindowThreadsMax, 1)
     windowed_kernel(const __grid_constant__ WorkPlan plan) {
@@ -1631,10 +1639,11 @@ __global__ void __launch_bounds__(kAlgorithm == 1 ? zhs_threads_max<Amp, kPass>(
   // this CTA's list of the deferred pairs of its current item (kPass 1: of
   // all its items, from `used` on; kPass 2: of the items it projects in full)
   unsigned* const deferred_list =
-      kPass == 2 ? plan.drain_deferred + static_cast<size_t>(blockIdx.x) * plan.deferred_stride
+      kPass >= 2 ? plan.drain_deferred + static_cast<size_t>(blockIdx.x) * plan.deferred_stride
       : kPass == 1 ? plan.deferred + static_cast<size_t>(blockIdx.x) * plan.deferred_capacity
                    : plan.deferred + static_cast<size_t>(blockIdx.x) * plan.deferred_stride;
   uint32_t used = 0;  // kPass 1: entries of the list taken by earlier items
+  bool full = false;  // kPass 1: the list overflowed; later items are handed back
   Counts c;
   for (;;) {
     __syncthreads();
@@ -1652,11 +1661,12 @@ __global__ void __launch_bounds__(kAlgorithm == 1 ? zhs_threads_max<Amp, kPass>(
     uint64_t const track_count = valid < ev.last_track ? valid : ev.last_track;
     uint64_t const begin = ev.first_track + slice_chunk * ev.chunk_size;
     ItemState state{blockIdx.x, used, 0u, 0u};
-    if constexpr (kPass == 2) {
+    if constexpr (kPass >= 2) {
       state = plan.item_state[item];
-      if (!state.redo && state.count == 0u) continue;  // done by the first pass
+      if (kPass == 2 && (state.redo || state.count == 0u)) continue;  // nothing to drain
+      if (kPass == 3 && !state.redo) continue;                          // done by passes 1-2
     }
-    bool const drain_only = kPass == 2 && !state.redo;
+    bool const drain_only = kPass == 2;
     if (begin >= track_count) {
       if (kPass == 1 && threadIdx.x == 0) plan.item_state[item] = state;
       continue;
@@ -1664,7 +1674,7 @@ __global__ void __launch_bounds__(kAlgorithm == 1 ? zhs_threads_max<Amp, kPass>(
     uint64_t const end = begin + ev.chunk_size < track_count ? begin + ev.chunk_size : track_count;
     uint64_t const bins = ev.observers[algorithm][oi].bins;
     uint32_t const width = static_cast<uint32_t>(bins < ev.window ? bins : ev.window);
-    if (kPass == 1 && bins > width) {  // checked adds past the window: the second pass
+    if (kPass == 1 && (full || bins > width)) {  // handed back unprojected
       if (threadIdx.x == 0) {
         plan.item_state[item] = ItemState{blockIdx.x, used, 0u, 1u};
         if (plan.handbacks) atomicAdd(plan.handbacks, 1ull);
@@ -1772,6 +1782,7 @@ __global__ void __launch_bounds__(kAlgorithm == 1 ? zhs_threads_max<Amp, kPass>(
       n = drain_only ? state.count : deferred_total;
       if (kPass == 1 && static_cast<uint64_t>(used) + n > plan.deferred_capacity) {
         redo = true;
+        full = true;
         break;
       }
       unsigned const* const list =
@@ -1964,17 +1975,22 @@ cudaError_t windowed_launch(WorkPlan const& plan, int ctas, int threads, cudaStr
   return cudaGetLastError();
 }
 
-// The two passes of a fixed-point ZHS launch, one after the other on the
-// stream; the second draws items from its own counter.
+// The passes of a two-pass fixed-point ZHS launch, one after the other on
+// the stream: the track loop, the drain, and the handed-back items in full;
+// the last two draw items from their own counter.
 template <class Amp, bool kPre>
 cudaError_t windowed_two_pass(WorkPlan const& plan, int ctas, int threads, cudaStream_t stream) {
   cudaError_t err = windowed_launch<true, Amp, 1, kPre, 1>(plan, ctas, threads, stream);
   if (err != cudaSuccess) return err;
+  WorkPlan later = plan;
+  later.next_item = plan.drain_next_item;
   err = cudaMemsetAsync(plan.drain_next_item, 0, sizeof(unsigned), stream);
   if (err != cudaSuccess) return err;
-  WorkPlan second = plan;
-  second.next_item = plan.drain_next_item;
-  return windowed_launch<true, Amp, 1, kPre, 2>(second, ctas, threads, stream);
+  err = windowed_launch<true, Amp, 1, kPre, 2>(later, ctas, threads, stream);
+  if (err != cudaSuccess) return err;
+  err = cudaMemsetAsync(plan.drain_next_item, 0, sizeof(unsigned), stream);
+  if (err != cudaSuccess) return err;
+  return windowed_launch<true, Amp, 1, kPre, 3>(later, ctas, threads, stream);
 }
 
 template <bool kFixed, class Amp, int kAlgorithm>
@@ -2025,6 +2041,8 @@ int ctas_per_sm(int window, int threads) {
     probe(windowed_kernel<true, Amp, 1, true, 1>, zhs_block<Amp, 1>(threads), 1);
     probe(windowed_kernel<true, Amp, 1, false, 2>, zhs_block<Amp, 2>(threads), 1);
     probe(windowed_kernel<true, Amp, 1, true, 2>, zhs_block<Amp, 2>(threads), 1);
+    probe(windowed_kernel<true, Amp, 1, false, 3>, zhs_block<Amp, 3>(threads), 1);
+    probe(windowed_kernel<true, Amp, 1, true, 3>, zhs_block<Amp, 3>(threads), 1);
   }
   return worst;
 }
