@@ -1424,15 +1424,18 @@ constexpr int kZhsThreadsFloat = 768;
 constexpr int kZhsThreadsDouble = 384;
 // Two passes (fixed point): the track loop alone runs larger CTAs (FP32 768
 // threads, FP64 480: the most its 72-byte staging slots allow beside an
-// 8192-bin window), the drain pass 384.
+// 8192-bin window), the drain pass FP32 512 (ZHS 62.0 -> 60.7 ms on the 1e7 x
+// 160 workload against 384; 768 ran slower), FP64 384.  FP64 track loops of
+// 512 threads with unpadded 64-byte slots ran 110.3 ms against 96.2.
 constexpr int kZhsLoopThreadsFloat = 768;
 constexpr int kZhsLoopThreadsDouble = 480;
-constexpr int kZhsDrainThreads = 384;
+constexpr int kZhsDrainThreadsFloat = 512;
+constexpr int kZhsDrainThreadsDouble = 384;
 // kPass: 0 one pass; of a two-pass launch 1 the track loop, 2 the drain, 3
 // the handed-back items in full (as one pass).
 template <class Amp, int kPass = 0>
 constexpr int zhs_threads_max() {
-  return kPass == 2   ? kZhsDrainThreads
+  return kPass == 2   ? (sizeof(Amp) == sizeof(float) ? kZhsDrainThreadsFloat : kZhsDrainThreadsDouble)
          : kPass == 1 ? (sizeof(Amp) == sizeof(float) ? kZhsLoopThreadsFloat : kZhsLoopThreadsDouble)
                       : (sizeof(Amp) == sizeof(float) ? kZhsThreadsFloat : kZhsThreadsDouble);
 }
