@@ -1414,12 +1414,15 @@ __global__ void __launch_bounds__(kTileThreads) tiled_kernel(const __grid_consta
 
 // ---------------------------------------------------------------- windowed
 constexpr int kWindowThreadsMax = kWindowThreads;
-// Threads of a ZHS CTA.  Its drain's live state needs more registers than its
-// track loop (168 against 112 in FP32, 135 in FP64), so a CTA sized for the
-// drain runs 12 warps an SM.  Measured on the 1e7 x 160 workload (ms per ZHS
-// launch), FP32: 384 threads 96.8, 512 100.9, 576 97.3, 640 88.3, 768 79.9,
-// 832 82.7, 864 80.6 -- the track loop gains more from the warps than the
-// drain loses to its spills; FP64: 384 117.0, 480 128.5.
+// Threads of a CTA of the one-pass ZHS kernel (floating traces, the
+// no-allocation entry point, launches past the two-pass storage cap, and the
+// third pass of two-pass launches).  Its drain's live state needs more
+// registers than its track loop (168 against 112 in FP32, 135 in FP64), so a
+// CTA sized for the drain runs 12 warps an SM.  Measured on the 1e7 x 160
+// workload in one pass (ms per ZHS launch), FP32: 384 threads 96.8, 512
+// 100.9, 576 97.3, 640 88.3, 768 79.9, 832 82.7, 864 80.6 -- the track loop
+// gains more from the warps than the drain loses to its spills; FP64: 384
+// 117.0, 480 128.5.
 constexpr int kZhsThreadsFloat = 768;
 constexpr int kZhsThreadsDouble = 384;
 // Two passes (fixed point): the track loop alone runs larger CTAs (FP32 768
