@@ -1414,7 +1414,9 @@ void set_global_error(char const* message) { g_last_error = message; }
 
 extern "C" {
 
-const char* c8r_version(void) { return "c8radio-b200 1.0 (sm_100a)"; }
+// Part of the tuning cache's key: raised whenever the kernels' launch shapes
+// change, so that a tile tuned for earlier kernels is not applied to these.
+const char* c8r_version(void) { return "c8radio-b200 1.1 (sm_100a)"; }
 
 const char* c8r_last_error(const c8r_accumulator* handle) {
   if (handle == nullptr) return g_last_error.c_str();
